@@ -1,0 +1,198 @@
+/* rt_trace.h — C ABI of the B200 software ray-traversal engine.
+ *
+ * The engine takes over renderlab's software BVH traversal: the ray-query seam that its non-RT
+ * GI, shadow and reflection passes call (shaders/gi_rays_software.wgsl:280-291 and
+ * shaders/reflections_software_bvh4.wgsl:140-207), over the packed u32 geometry buffers that
+ * src/gi_bvh.rs and src/reflection_software.rs write. Scenes are uploaded as those words,
+ * verbatim; rays go in as 32-byte records and hits come out as the seam's hit records.
+ *
+ * Conventions: every function returns rt_status; on failure rt_get_last_error() describes it.
+ * Device pointers are CUDA device addresses on the context's device; `stream` is a
+ * cudaStream_t (NULL: the legacy default stream). No call traps or hangs the GPU: stack
+ * overflows and device waits are bounded and reported through rt_get_stats().
+ */
+#ifndef RT_TRACE_H
+#define RT_TRACE_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RT_ABI_VERSION 1u
+
+typedef enum rt_status {
+  RT_OK = 0,
+  RT_ERR_INVALID_ARG = 1,    /* null pointer, bad size, unknown enum */
+  RT_ERR_LAYOUT = 2,         /* packed words fail validation (src/gi_bvh.rs:33-36 InvalidInput) */
+  RT_ERR_OOM = 3,            /* device or host allocation refused / over the HBM budget */
+  RT_ERR_STACK_OVERFLOW = 4, /* a traversal stack was full; the push was dropped and counted */
+  RT_ERR_TIMEOUT = 5,        /* a bounded device or host wait gave up */
+  RT_ERR_CUDA = 6,           /* a CUDA runtime call failed (src/lib.rs:138-160 Error::Fault) */
+  RT_ERR_BUSY = 7,           /* the serving queue is full or closed */
+  RT_ERR_UNSUPPORTED = 8     /* option not available for this layout / kernel */
+} rt_status;
+
+/* The two packed layouts. */
+typedef enum rt_layout {
+  RT_LAYOUT_GI = 0,         /* gi_geometry: 16-word header, 32-word instances (src/gi_bvh.rs:19-25) */
+  RT_LAYOUT_REFLECTION = 1  /* rl_geometry: 8-word header, 24-word instances (reflection_software.rs:38-42) */
+} rt_layout;
+
+/* Query modes: gi_traverse's mode argument (gi_rays_software.wgsl:214-217). For the reflection
+ * layout CLOSEST is rs_closest and either any-hit mode is rs_blocked. */
+typedef enum rt_mode {
+  RT_CLOSEST = 0,     /* gi_closest / rs_closest */
+  RT_ANY_SKY = 1,     /* gi_visible (any hit; instances flagged "casts no shadow" skipped) */
+  RT_ANY_CASTERS = 2  /* gi_visible_within / rs_blocked */
+} rt_mode;
+
+/* Traversal kernels. PLAIN is the loop-for-loop transcription of the WGSL (bit-exact with it);
+ * FAST runs the same arithmetic in a scheduled kernel (bit-exact with PLAIN); WIDE8 traverses
+ * the engine's compressed 8-wide BVH with watertight triangle tests and an FP64 re-test of
+ * near ties (same hit ids except near ties; t within 1e-5 relative of FP64). */
+typedef enum rt_kernel {
+  RT_KERNEL_PLAIN = 0,
+  RT_KERNEL_FAST = 1,
+  RT_KERNEL_WIDE8 = 2
+} rt_kernel;
+
+/* One ray, 32 bytes: origin, tmin, direction (need not be unit length), tmax. */
+typedef struct rt_ray {
+  float o[3];
+  float tmin;
+  float d[3];
+  float tmax;
+} rt_ray;
+
+/* Reflection closest hit, 20 bytes: t and the hardware ray-query record
+ * (placement slot + 1, primitive, u bits, v bits); rec[0] == 0 is a miss
+ * (reflections_software_bvh4.wgsl:42,90). */
+typedef struct rt_hit {
+  float t;
+  uint32_t rec[4];
+} rt_hit;
+
+/* GI closest hit, 40 bytes: GiHit (gi_rays_software.wgsl:19). inst == 0xffffffff is a miss;
+ * tri holds the three position indices, or (primitive, 0, 0) for meshes with a primitive table;
+ * normal is unit_normal of the source-winding normal in world space. */
+typedef struct rt_gi_hit {
+  float t;
+  uint32_t inst;
+  uint32_t tri[3];
+  float bary[2];
+  float normal[3];
+} rt_gi_hit;
+
+/* Any-hit results are one uint32 per ray: 1 when something blocks the ray, else 0
+ * (gi_visible returns the negation). */
+
+typedef struct rt_ctx rt_ctx;
+typedef struct rt_scene rt_scene;
+typedef struct rt_blas rt_blas;
+
+typedef struct rt_stats {
+  uint64_t rays_traced;
+  uint64_t stack_overflows; /* pushes dropped because a stack was full */
+  uint64_t launches;
+  uint64_t scene_bytes;     /* device bytes held by uploaded scenes */
+} rt_stats;
+
+/* ---- context ---- */
+uint32_t rt_abi_version(void);
+rt_status rt_ctx_create(int device, rt_ctx** out);
+void rt_ctx_destroy(rt_ctx* ctx);
+const char* rt_get_last_error(const rt_ctx* ctx);
+rt_status rt_get_stats(rt_ctx* ctx, rt_stats* out);
+/* Runs a small device kernel that reports the device's arithmetic conventions (signed-zero
+ * min/max, correctly rounded reciprocal and square root) as 16 result words. */
+rt_status rt_selftest(rt_ctx* ctx, uint32_t out[16]);
+
+/* ---- scenes: packed words in, device-resident scene out ----
+ * Replaces the renderer's `queue.write_buffer` of gi_geometry / rl_geometry
+ * (gi_cache.rs:4480-4484, primary_ray_gpu.rs:3672-3709). The words are validated (ranges,
+ * acyclic trees) before upload so that no traversal can read outside them. */
+rt_status rt_scene_upload(rt_ctx* ctx, rt_layout layout, const uint32_t* words, size_t n_words,
+                          rt_scene** out);
+/* Rewrites the leading words (header, instance records, top level) of an uploaded scene, as
+ * the renderer does each frame when transforms change. The mesh words must be unchanged. */
+/* The upload's admission check alone, on the host (no device needed). info: instances,
+ * top-level base, root, distinct triangles, distinct BLAS nodes, deepest BLAS, deepest top
+ * level, 0. */
+rt_status rt_scene_validate(rt_layout layout, const uint32_t* words, size_t n_words, uint32_t info[8],
+                            char* err, size_t err_len);
+rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* words,
+                                  size_t n_words);
+rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene);
+size_t rt_scene_device_bytes(const rt_scene* scene);
+
+/* ---- traversal ----
+ * rt_trace: the seam. d_rays holds n rt_ray; d_hits receives n rt_gi_hit (GI closest),
+ * n rt_hit (reflection closest) or n uint32 (any-hit). Asynchronous on `stream`; allocates
+ * nothing. */
+rt_status rt_trace(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, const rt_ray* d_rays,
+                   void* d_hits, uint32_t n, void* stream);
+/* rt_trace with an explicit kernel (rt_kernel) and, for FAST / WIDE8, an optional device
+ * permutation (d_order[i] is the ray traced by thread i; NULL: identity). */
+rt_status rt_trace_ex(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
+                      const rt_ray* d_rays, const uint32_t* d_order, void* d_hits, uint32_t n,
+                      void* stream);
+/* Host-buffer form: copies rays in and hits out through the context's pinned staging and
+ * device buffers (grown on first use, or sized ahead by rt_ctx_reserve), pipelined in chunks
+ * over two streams. Returns when the hits are in h_hits. */
+rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
+                        const rt_ray* h_rays, void* h_hits, uint32_t n);
+rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays);
+
+/* ---- host builders (the CPU side of the path: crates/asset/src/near_field.rs:172-541,
+ * src/instance_bvh.rs:162-460, src/gi_bvh.rs, src/reflection_software.rs) ---- */
+#define RT_BUILD_SAH 0u    /* build_bvh_sah (near_field.rs:184): binned SAH, median past depth 15 */
+#define RT_BUILD_MEDIAN 1u /* build_bvh (near_field.rs:172) */
+rt_status rt_blas_build(const float* positions, uint32_t n_positions, const uint32_t* indices,
+                        uint32_t n_indices, uint32_t build_flags, rt_blas** out);
+/* info: nodes, leaves, positions, indices, root, depth */
+rt_status rt_blas_info(const rt_blas* blas, uint32_t info[6]);
+/* The 16-word runtime node records (gi_bvh.rs:191-203), 16 * nodes words. */
+rt_status rt_blas_nodes(const rt_blas* blas, uint32_t* out);
+/* The reordered triangle-list indices (near_field.rs:380-400), `indices` words. */
+rt_status rt_blas_indices(const rt_blas* blas, uint32_t* out);
+/* refit_bvh (near_field.rs:445-478): same vertices, new positions. */
+rt_status rt_blas_refit(rt_blas* blas, const float* positions, uint32_t n_positions);
+void rt_blas_free(rt_blas* blas);
+
+/* One placement for the packers. model: object-to-world, 3 rows of 4; rows: the world-to-object
+ * rows the record carries (words 0-11). GI: near_base is word 23 and extra words 24-31
+ * (identity, map, map length, flags bit0 = casts no shadow, -, placement); word 28 (primitive
+ * table) is derived. Reflection: slot is word 21, casts_shadow selects word 22. */
+typedef struct rt_instance {
+  float model[12];
+  float rows[12];
+  uint32_t mesh;
+  uint32_t slot;
+  uint32_t casts_shadow;
+  uint32_t near_base;
+  uint32_t extra[8];
+} rt_instance;
+
+/* Packs meshes and instances into the layout's words (gi_bvh.rs:151-274 + gi_cache.rs:4388-4488;
+ * reflection_software.rs:285-388 + primary_ray_gpu.rs:3640-3662), with the instance top level
+ * (instance_bvh.rs:162-220; tlas_mode -1 default (>= 40 instances), 0 off, 1 on).
+ * mesh_primitives[m] != 0 adds the GI primitive table for mesh m (source indices given).
+ * Call with out_words NULL to learn the size in *n_words. */
+rt_status rt_pack_scene(rt_layout layout, const rt_blas* const* meshes, uint32_t n_meshes,
+                        const float* const* mesh_positions, const uint32_t* const* mesh_indices,
+                        const uint32_t* mesh_n_indices, const uint32_t* mesh_primitives,
+                        const rt_instance* instances, uint32_t n_instances, int tlas_mode,
+                        uint32_t* out_words, size_t* n_words);
+
+/* Instance top level alone (instance_bvh.rs:346-366): boxes are 6 floats (lo xyz, hi xyz).
+ * Call with out NULL to learn the size. */
+rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);
+rt_status rt_tlas_refit(uint32_t* nodes, size_t n_words, const float* boxes, uint32_t n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RT_TRACE_H */

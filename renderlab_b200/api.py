@@ -1,0 +1,389 @@
+"""Python host side of the engine, over the C ABI in ``include/rt_trace.h``.
+
+Mirrors renderlab's ray-query seam (shaders/gi_rays_software.wgsl:280-291 and
+shaders/reflections_software_bvh4.wgsl:206-207) for batches of rays:
+
+* ``gi_closest(scene, rays)``          -> GI hits (t, instance, triangle, barycentrics, normal)
+* ``gi_visible(scene, o, d)``          -> True where nothing blocks (tmin 0, tmax 1e20)
+* ``gi_visible_within(scene, o, d, tmax)``
+* ``rs_trace(scene, rays, any_hit)``   -> reflection records (slot + 1, primitive, u, v) and t
+* ``rs_closest`` / ``rs_blocked``
+
+Device buffers are torch CUDA tensors (PyTorch is only the allocator and stream source here);
+``Engine.trace_host`` takes host arrays and copies through the library's pipelined staging.
+Every traversal runs in ``_lib/librt_trace.so``; there is no CPU fallback, and importing this
+module on a machine without the library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "_lib" / "librt_trace.so"
+
+LAYOUT_GI, LAYOUT_REFLECTION = 0, 1
+CLOSEST, ANY_SKY, ANY_CASTERS = 0, 1, 2
+KERNELS = {"plain": 0, "fast": 1, "wide8": 2}
+STATUS = {0: "OK", 1: "INVALID_ARG", 2: "LAYOUT", 3: "OOM", 4: "STACK_OVERFLOW", 5: "TIMEOUT",
+          6: "CUDA", 7: "BUSY", 8: "UNSUPPORTED"}
+GI_HIT_WORDS, RS_HIT_WORDS = 10, 5
+MISS = 0xFFFFFFFF
+
+_u32p = ctypes.POINTER(ctypes.c_uint32)
+_f32p = ctypes.POINTER(ctypes.c_float)
+_vp = ctypes.c_void_p
+
+
+class RtError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+
+
+class RtStats(ctypes.Structure):
+    _fields_ = [("rays_traced", ctypes.c_uint64), ("stack_overflows", ctypes.c_uint64),
+                ("launches", ctypes.c_uint64), ("scene_bytes", ctypes.c_uint64)]
+
+
+class RtInstance(ctypes.Structure):
+    _fields_ = [("model", ctypes.c_float * 12), ("rows", ctypes.c_float * 12), ("mesh", ctypes.c_uint32),
+                ("slot", ctypes.c_uint32), ("casts_shadow", ctypes.c_uint32), ("near_base", ctypes.c_uint32),
+                ("extra", ctypes.c_uint32 * 8)]
+
+
+EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",
+           "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
+           "rt_scene_device_bytes", "rt_scene_validate", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve",
+           "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
+           "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
+
+_lib = None
+
+
+def lib() -> ctypes.CDLL:
+    """The loaded library (raises if it was never built: there is no fallback path)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m renderlab_b200.build` "
+                           "(the engine has no CPU fallback)")
+    L = ctypes.CDLL(str(LIB_PATH))
+    L.rt_abi_version.restype = ctypes.c_uint32
+    L.rt_ctx_create.argtypes = [ctypes.c_int, ctypes.POINTER(_vp)]
+    L.rt_ctx_destroy.argtypes = [_vp]
+    L.rt_ctx_destroy.restype = None
+    L.rt_get_last_error.argtypes = [_vp]
+    L.rt_get_last_error.restype = ctypes.c_char_p
+    L.rt_get_stats.argtypes = [_vp, ctypes.POINTER(RtStats)]
+    L.rt_selftest.argtypes = [_vp, _u32p]
+    L.rt_scene_upload.argtypes = [_vp, ctypes.c_int, _u32p, ctypes.c_size_t, ctypes.POINTER(_vp)]
+    L.rt_scene_validate.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, _u32p, ctypes.c_char_p, ctypes.c_size_t]
+    L.rt_scene_update_records.argtypes = [_vp, _vp, _u32p, ctypes.c_size_t]
+    L.rt_scene_release.argtypes = [_vp, _vp]
+    L.rt_scene_device_bytes.argtypes = [_vp]
+    L.rt_scene_device_bytes.restype = ctypes.c_size_t
+    L.rt_trace.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
+    L.rt_trace_ex.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]
+    L.rt_trace_host.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32]
+    L.rt_ctx_reserve.argtypes = [_vp, ctypes.c_uint32]
+    L.rt_blas_build.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_vp)]
+    L.rt_blas_info.argtypes = [_vp, _u32p]
+    L.rt_blas_nodes.argtypes = [_vp, _u32p]
+    L.rt_blas_indices.argtypes = [_vp, _u32p]
+    L.rt_blas_refit.argtypes = [_vp, _f32p, ctypes.c_uint32]
+    L.rt_blas_free.argtypes = [_vp]
+    L.rt_blas_free.restype = None
+    L.rt_pack_scene.argtypes = [ctypes.c_int, ctypes.POINTER(_vp), ctypes.c_uint32, ctypes.POINTER(_f32p),
+                                ctypes.POINTER(_u32p), _u32p, _u32p, ctypes.POINTER(RtInstance), ctypes.c_uint32,
+                                ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
+    L.rt_tlas_build.argtypes = [_f32p, ctypes.c_uint32, ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
+    L.rt_tlas_refit.argtypes = [_u32p, ctypes.c_size_t, _f32p, ctypes.c_uint32]
+    for name in EXPORTS:
+        if name not in ("rt_ctx_destroy", "rt_blas_free", "rt_abi_version", "rt_get_last_error",
+                        "rt_scene_device_bytes"):
+            getattr(L, name).restype = ctypes.c_int
+    _lib = L
+    return L
+
+
+def _np_ptr(a, t):
+    return a.ctypes.data_as(t)
+
+
+# ---------------------------------------------------------------- host builders
+
+class Blas:
+    """A BVH4-Q8 over one triangle mesh (near_field.rs build_bvh_sah / build_bvh)."""
+
+    def __init__(self, positions, indices, median: bool = False):
+        self.positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        self.indices = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        h = _vp()
+        st = lib().rt_blas_build(_np_ptr(self.positions, _f32p), len(self.positions), _np_ptr(self.indices, _u32p),
+                                 len(self.indices), 1 if median else 0, ctypes.byref(h))
+        if st != 0:
+            raise RtError(st, "BVH geometry needs a nonempty, finite triangle list")
+        self.h = h
+
+    def __del__(self):
+        if getattr(self, "h", None) and _lib is not None:
+            _lib.rt_blas_free(self.h)
+            self.h = None
+
+    def info(self) -> dict:
+        out = np.zeros(6, np.uint32)
+        lib().rt_blas_info(self.h, _np_ptr(out, _u32p))
+        return dict(zip(("nodes", "leaves", "positions", "indices", "root", "depth"), map(int, out)))
+
+    def nodes(self) -> np.ndarray:
+        out = np.zeros((self.info()["nodes"], 16), np.uint32)
+        lib().rt_blas_nodes(self.h, _np_ptr(out, _u32p))
+        return out
+
+    def bvh_indices(self) -> np.ndarray:
+        out = np.zeros(self.info()["indices"], np.uint32)
+        lib().rt_blas_indices(self.h, _np_ptr(out, _u32p))
+        return out
+
+    def refit(self, positions) -> None:
+        p = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        st = lib().rt_blas_refit(self.h, _np_ptr(p, _f32p), len(p))
+        if st != 0:
+            raise RtError(st, "refit needs finite positions of the same vertices")
+        self.positions = p
+
+
+def pack_scene(layout: int, meshes, instances, tlas_mode: int = -1, primitives=None) -> np.ndarray:
+    """Packed words of `layout` for meshes (list of Blas) placed by `instances`.
+
+    instances: object with ``model`` (N,3,4), ``rows`` (N,3,4), ``mesh`` (N,), and optionally
+    ``casts`` (N,) bool, ``slot`` (N,), ``near_base`` (N,), ``extra`` (N,8).
+    primitives: per mesh, whether the GI layout carries its primitive table.
+    """
+    n = len(instances.mesh)
+    arr = (RtInstance * max(n, 1))()
+    model = np.ascontiguousarray(instances.model, np.float32).reshape(n, 12)
+    rows = np.ascontiguousarray(instances.rows, np.float32).reshape(n, 12)
+    casts = getattr(instances, "casts", None)
+    slot = getattr(instances, "slot", None)
+    near = getattr(instances, "near_base", None)
+    extra = getattr(instances, "extra", None)
+    for i in range(n):
+        rec = arr[i]
+        ctypes.memmove(rec.model, model[i].ctypes.data, 48)
+        ctypes.memmove(rec.rows, rows[i].ctypes.data, 48)
+        rec.mesh = int(instances.mesh[i])
+        rec.slot = int(slot[i]) if slot is not None else i
+        rec.casts_shadow = int(bool(casts[i])) if casts is not None else 1
+        rec.near_base = int(near[i]) if near is not None else 0
+        if extra is not None:
+            for k in range(8):
+                rec.extra[k] = int(extra[i][k])
+        elif casts is not None and layout == LAYOUT_GI:
+            rec.extra[3] = 0 if casts[i] else 1
+    m = len(meshes)
+    handles = (_vp * max(m, 1))(*[b.h for b in meshes])
+    pos_ptrs = (_f32p * max(m, 1))(*[_np_ptr(b.positions, _f32p) for b in meshes])
+    idx_ptrs = (_u32p * max(m, 1))(*[_np_ptr(b.indices, _u32p) for b in meshes])
+    nidx = np.array([len(b.indices) for b in meshes] or [0], np.uint32)
+    prim = np.array([int(bool(p)) for p in (primitives or [False] * m)] or [0], np.uint32)
+    size = ctypes.c_size_t(0)
+    L = lib()
+    args = (layout, handles, m, pos_ptrs, idx_ptrs, _np_ptr(nidx, _u32p), _np_ptr(prim, _u32p), arr, n, tlas_mode)
+    st = L.rt_pack_scene(*args, None, ctypes.byref(size))
+    if st != 0:
+        raise RtError(st, "packing failed (singular transform, bad mesh index or unmappable triangles)")
+    out = np.zeros(size.value, np.uint32)
+    st = L.rt_pack_scene(*args, _np_ptr(out, _u32p), ctypes.byref(size))
+    if st != 0:
+        raise RtError(st, "packing failed")
+    return out
+
+
+def validate(layout: int, words) -> dict:
+    """The upload admission check on the host; raises RtError(LAYOUT) with the reason."""
+    w = np.ascontiguousarray(words, np.uint32)
+    info = np.zeros(8, np.uint32)
+    err = ctypes.create_string_buffer(256)
+    st = lib().rt_scene_validate(layout, _np_ptr(w, _u32p), len(w), _np_ptr(info, _u32p), err, 256)
+    if st != 0:
+        raise RtError(st, err.value.decode())
+    return dict(zip(("instances", "top", "root", "triangles", "nodes", "blas_depth", "top_depth"), map(int, info)))
+
+
+def tlas_build(boxes, sah: bool = True) -> np.ndarray:
+    b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    size = ctypes.c_size_t(0)
+    st = lib().rt_tlas_build(_np_ptr(b, _f32p), len(b), int(sah), None, ctypes.byref(size))
+    if st != 0:
+        raise RtError(st, "top level needs at least two boxes")
+    out = np.zeros(size.value, np.uint32)
+    lib().rt_tlas_build(_np_ptr(b, _f32p), len(b), int(sah), _np_ptr(out, _u32p), ctypes.byref(size))
+    return out
+
+
+def tlas_refit(nodes, boxes) -> np.ndarray:
+    nodes = np.ascontiguousarray(nodes, np.uint32).copy()
+    b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    st = lib().rt_tlas_refit(_np_ptr(nodes, _u32p), len(nodes), _np_ptr(b, _f32p), len(b))
+    if st != 0:
+        raise RtError(st, "refit needs at least two boxes")
+    return nodes
+
+
+# ---------------------------------------------------------------- device side
+
+def hit_words(layout: int, mode: int) -> int:
+    if mode != CLOSEST:
+        return 1
+    return GI_HIT_WORDS if layout == LAYOUT_GI else RS_HIT_WORDS
+
+
+@dataclass
+class Scene:
+    engine: "Engine"
+    handle: int
+    layout: int
+    n_words: int
+
+    def release(self):
+        if self.handle:
+            self.engine._check(lib().rt_scene_release(self.engine.ctx, self.handle))
+            self.handle = None
+
+    def update_records(self, words):
+        w = np.ascontiguousarray(words, np.uint32)
+        self.engine._check(lib().rt_scene_update_records(self.engine.ctx, self.handle, _np_ptr(w, _u32p), len(w)))
+
+    @property
+    def device_bytes(self) -> int:
+        return int(lib().rt_scene_device_bytes(self.handle))
+
+
+class Engine:
+    """One context on one CUDA device."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+        h = _vp()
+        st = lib().rt_ctx_create(device, ctypes.byref(h))
+        if st != 0:
+            raise RtError(st, f"cannot create a context on device {device}")
+        self.ctx = h
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            lib().rt_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        if _lib is not None:
+            self.close()
+
+    def _check(self, st: int):
+        if st != 0:
+            raise RtError(st, lib().rt_get_last_error(self.ctx).decode())
+
+    def selftest(self) -> np.ndarray:
+        out = np.zeros(16, np.uint32)
+        self._check(lib().rt_selftest(self.ctx, _np_ptr(out, _u32p)))
+        return out
+
+    def stats(self) -> dict:
+        s = RtStats()
+        self._check(lib().rt_get_stats(self.ctx, ctypes.byref(s)))
+        return {f: int(getattr(s, f)) for f, _ in RtStats._fields_}
+
+    def upload(self, layout: int, words) -> Scene:
+        w = np.ascontiguousarray(words, np.uint32)
+        h = _vp()
+        self._check(lib().rt_scene_upload(self.ctx, layout, _np_ptr(w, _u32p), len(w), ctypes.byref(h)))
+        return Scene(self, h, layout, len(w))
+
+    def trace(self, scene: Scene, rays, mode: int = CLOSEST, kernel: str = "plain", order=None, hits=None,
+              stream=None):
+        """Trace a torch CUDA tensor of rays (n, 8) float32; returns the int32 hit tensor."""
+        import torch
+        assert rays.is_cuda and rays.dtype == torch.float32 and rays.is_contiguous()
+        n = rays.shape[0]
+        words = hit_words(scene.layout, mode)
+        if hits is None:
+            hits = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=rays.device)
+        s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+        self._check(lib().rt_trace_ex(self.ctx, scene.handle, mode, KERNELS[kernel], rays.data_ptr(),
+                                      order.data_ptr() if order is not None else None, hits.data_ptr(), n, s))
+        return hits
+
+    def trace_host(self, scene: Scene, rays, mode: int = CLOSEST, kernel: str = "plain", out=None):
+        """Trace host rays (numpy or pinned torch CPU tensor, (n, 8) float32) into host hits."""
+        n = len(rays)
+        words = hit_words(scene.layout, mode)
+        if out is None:
+            out = np.zeros((n, words) if words > 1 else (n,), np.uint32)
+        rp = rays.data_ptr() if hasattr(rays, "data_ptr") else rays.ctypes.data
+        hp = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        self._check(lib().rt_trace_host(self.ctx, scene.handle, mode, KERNELS[kernel], rp, hp, n))
+        return out
+
+    def reserve(self, max_rays: int):
+        self._check(lib().rt_ctx_reserve(self.ctx, max_rays))
+
+
+# ---------------------------------------------------------------- the seam, batched
+
+def _rays(origin, direction, tmin, tmax):
+    import torch
+    o = torch.as_tensor(origin, dtype=torch.float32)
+    d = torch.as_tensor(direction, dtype=torch.float32)
+    n = o.shape[0]
+    r = torch.empty((n, 8), dtype=torch.float32, device=o.device)
+    r[:, 0:3] = o
+    r[:, 3] = torch.as_tensor(tmin, dtype=torch.float32, device=o.device)
+    r[:, 4:7] = d
+    r[:, 7] = torch.as_tensor(tmax, dtype=torch.float32, device=o.device)
+    return r
+
+
+def decode_gi(hits) -> dict:
+    """Split (n, 10) GI hit words into named fields (torch int32 tensor or numpy)."""
+    h = hits
+    f = h.view(np.float32) if isinstance(h, np.ndarray) else h.view(__import__("torch").float32)
+    return dict(t=f[:, 0], inst=h[:, 1], tri=h[:, 2:5], bary=f[:, 5:7], normal=f[:, 7:10])
+
+
+def gi_closest(engine: Engine, scene: Scene, origin, direction, tmin, tmax, kernel="plain") -> dict:
+    """gi_closest (gi_rays_software.wgsl:280-282) for a batch of rays on the device."""
+    return decode_gi(engine.trace(scene, _rays(origin, direction, tmin, tmax), CLOSEST, kernel))
+
+
+def gi_visible(engine: Engine, scene: Scene, origin, direction, kernel="plain"):
+    """gi_visible (gi_rays_software.wgsl:285-287): sky visibility along [0, 1e20)."""
+    return engine.trace(scene, _rays(origin, direction, 0.0, 1e20), ANY_SKY, kernel) == 0
+
+
+def gi_visible_within(engine: Engine, scene: Scene, origin, direction, tmax, kernel="plain"):
+    """gi_visible_within (gi_rays_software.wgsl:289-291): opaque casters within tmax."""
+    return engine.trace(scene, _rays(origin, direction, 0.0, tmax), ANY_CASTERS, kernel) == 0
+
+
+def rs_trace(engine: Engine, scene: Scene, origin, direction, tmin, tmax, any_hit=False, kernel="plain"):
+    """rs_trace (reflections_software_bvh4.wgsl:140): (t, record) or the blocked flags."""
+    import torch
+    h = engine.trace(scene, _rays(origin, direction, tmin, tmax), ANY_CASTERS if any_hit else CLOSEST, kernel)
+    if any_hit:
+        return h != 0
+    return h[:, 0].view(torch.float32), h[:, 1:5]
+
+
+def rs_closest(engine, scene, origin, direction, tmin, tmax, kernel="plain"):
+    """rs_closest (reflections_software_bvh4.wgsl:206): the hit record (slot+1, prim, u, v)."""
+    return rs_trace(engine, scene, origin, direction, tmin, tmax, False, kernel)[1]
+
+
+def rs_blocked(engine, scene, origin, direction, tmin, tmax, kernel="plain"):
+    """rs_blocked (reflections_software_bvh4.wgsl:207)."""
+    return rs_trace(engine, scene, origin, direction, tmin, tmax, True, kernel)

@@ -1,0 +1,98 @@
+// Host side of the engine: the CPU builders and packers that produce the packed words the
+// traversal kernels read, and the validator that admits a buffer to the device.
+#pragma once
+#include <array>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <string>
+#include <vector>
+
+namespace rtb {
+
+constexpr uint32_t LEAF = 0x80000000u;
+constexpr uint32_t EMPTY = 0xffffffffu;
+constexpr uint32_t LEAF_TRIANGLES = 8;  // near_field.rs:23
+constexpr uint32_t MAX_SAH_DEPTH = 15;  // near_field.rs:178
+constexpr uint32_t STACK_DEPTH = 48;    // gi_rays_software.wgsl:22, reflections_software_bvh4.wgsl:12
+
+inline uint32_t as_bits(float f) { uint32_t u; std::memcpy(&u, &f, 4); return u; }
+inline float as_float(uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; }
+// f32::min / f32::max over non-NaN operands (the first operand wins a tie).
+inline float lo_of(float a, float b) { return b < a ? b : a; }
+inline float hi_of(float a, float b) { return b > a ? b : a; }
+inline int32_t order_key(float f) {  // f32::total_cmp
+  int32_t x; std::memcpy(&x, &f, 4);
+  return x ^ (int32_t)(((uint32_t)(x >> 31)) >> 1);
+}
+
+struct Aabb {
+  float lo[3], hi[3];
+  static Aabb empty() { return {{INFINITY, INFINITY, INFINITY}, {-INFINITY, -INFINITY, -INFINITY}}; }
+  void grow(const float* p) {
+    for (int a = 0; a < 3; ++a) lo[a] = lo_of(lo[a], p[a]), hi[a] = hi_of(hi[a], p[a]);
+  }
+  void grow(const Aabb& b) {
+    for (int a = 0; a < 3; ++a) lo[a] = lo_of(lo[a], b.lo[a]), hi[a] = hi_of(hi[a], b.hi[a]);
+  }
+};
+
+// A one-level BVH4 with 8-bit child boxes in its 16-word runtime form: origin[3], step[3],
+// children[4], lower byte planes[3], upper byte planes[3] (gi_bvh.rs:191-203).
+struct Blas {
+  std::vector<uint32_t> nodes;    // 16 words a node, postorder (root last)
+  std::vector<uint32_t> leaves;   // (index offset, index count) a leaf
+  std::vector<float> positions;   // xyz a vertex (the input positions, unchanged)
+  std::vector<uint32_t> indices;  // reordered triangle list
+  uint32_t root = EMPTY;
+  Aabb bounds;                    // every position (gi_bvh.rs:70)
+  size_t node_count() const { return nodes.size() / 16; }
+  size_t leaf_count() const { return leaves.size() / 2; }
+};
+
+bool build_blas(const float* pos, size_t npos, const uint32_t* idx, size_t nidx, bool sah, Blas& out,
+                std::string& err);
+bool build_blas_sah(const float* pos, size_t npos, const uint32_t* idx, size_t nidx, Blas& out,
+                    std::string& err);
+size_t blas_depth(const Blas& b, uint32_t child);
+bool refit_blas(Blas& b, const float* pos, size_t npos, std::string& err);
+void quantize_node(const uint32_t* children, const Aabb* boxes, int n, uint32_t* w16);
+
+// Instance top level (instance_bvh.rs)
+size_t tlas_reserve(size_t instances);
+std::vector<uint32_t> tlas_build(const std::vector<Aabb>& boxes, bool sah);
+void tlas_refit(uint32_t* nodes, const std::vector<Aabb>& boxes);
+void tlas_place(std::vector<uint32_t>& words, size_t header, size_t stride, size_t slots, int mode);
+
+struct Placement {
+  float model[12];
+  float rows[12];
+  uint32_t mesh, slot, casts_shadow, near_base;
+  uint32_t extra[8];
+};
+struct MeshRef {
+  const Blas* blas;
+  const float* positions;  // source positions (reflection triangles are written from them)
+  const uint32_t* indices; // source triangle list (primitive ids)
+  size_t n_indices;
+  bool primitives;         // GI: append the primitive table
+};
+bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst, int tlas_mode,
+             std::vector<uint32_t>& out, std::string& err);
+bool pack_reflection(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst,
+                     int tlas_mode, std::vector<uint32_t>& out, std::string& err);
+
+// What a validated buffer holds, for the launchers and the derived layouts.
+struct SceneInfo {
+  uint32_t layout = 0;
+  uint32_t instances = 0;
+  uint32_t top = 0;           // top-level base word (0: flat list)
+  uint32_t root = 0;
+  size_t triangles = 0;       // distinct mesh triangles
+  size_t nodes = 0;           // distinct BLAS nodes
+  uint32_t max_blas_depth = 0;
+  uint32_t max_top_depth = 0;
+};
+bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& info, std::string& err);
+
+}  // namespace rtb

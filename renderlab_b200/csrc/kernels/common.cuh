@@ -1,0 +1,78 @@
+// Shared device helpers for the traversal kernels.
+//
+// Arithmetic convention of the bit-exact kernels (PLAIN, FAST): every multiply, add, subtract
+// and reciprocal is an explicit round-to-nearest intrinsic (__fmul_rn, __fadd_rn, __fsub_rn,
+// __frcp_rn), which nvcc never contracts into an FMA, so each WGSL operation rounds on its own.
+// Sums run left to right; cross products use the textbook component order. min/max are
+// fminf/fmaxf.
+#pragma once
+#include <cstdint>
+
+#define RT_DEV __device__ __forceinline__
+
+namespace rtk {
+
+constexpr uint32_t LEAF = 0x80000000u;
+constexpr uint32_t EMPTY = 0xffffffffu;
+constexpr float BIG = 3.4028235e38f;
+constexpr uint32_t STACK = 48;
+
+struct F3 {
+  float x, y, z;
+};
+
+RT_DEV float mul(float a, float b) { return __fmul_rn(a, b); }
+RT_DEV float add(float a, float b) { return __fadd_rn(a, b); }
+RT_DEV float sub(float a, float b) { return __fsub_rn(a, b); }
+RT_DEV F3 sub3(F3 a, F3 b) { return {sub(a.x, b.x), sub(a.y, b.y), sub(a.z, b.z)}; }
+RT_DEV float dot3(F3 a, F3 b) { return add(add(mul(a.x, b.x), mul(a.y, b.y)), mul(a.z, b.z)); }
+RT_DEV F3 cross3(F3 a, F3 b) {
+  return {sub(mul(a.y, b.z), mul(a.z, b.y)), sub(mul(a.z, b.x), mul(a.x, b.z)), sub(mul(a.x, b.y), mul(a.y, b.x))};
+}
+// dot(r, vec4(p, 1.0))
+RT_DEV float dot4p(float r0, float r1, float r2, float r3, F3 p) {
+  return add(add(add(mul(r0, p.x), mul(r1, p.y)), mul(r2, p.z)), mul(r3, 1.0f));
+}
+RT_DEV float next_up(float t) { return __uint_as_float(__float_as_uint(t) + 1u); }
+
+// gi_safe_inverse / rs_inverse: 1/d with |d| < 1e-30 replaced by +-1e-30 (sign of d >= 0).
+RT_DEV float safe_rcp(float d) {
+  float tiny = d >= 0.0f ? 1e-30f : -1e-30f;
+  return __frcp_rn(fabsf(d) < 1e-30f ? tiny : d);
+}
+RT_DEV F3 safe_inverse(F3 d) { return {safe_rcp(d.x), safe_rcp(d.y), safe_rcp(d.z)}; }
+
+// gi_slab_near / rs_box: entry distance clamped to tmin, or BIG when the slabs miss.
+RT_DEV float slab_near(F3 o, F3 inv, F3 lo, F3 hi, float tmin, float tmax) {
+  float ax = mul(sub(lo.x, o.x), inv.x), ay = mul(sub(lo.y, o.y), inv.y), az = mul(sub(lo.z, o.z), inv.z);
+  float bx = mul(sub(hi.x, o.x), inv.x), by = mul(sub(hi.y, o.y), inv.y), bz = mul(sub(hi.z, o.z), inv.z);
+  float near = fmaxf(fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz)), tmin);
+  float far = fminf(fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz)), tmax);
+  return near <= far ? near : BIG;
+}
+
+RT_DEV uint32_t ld(const uint32_t* __restrict__ w, size_t i) { return __ldg(w + i); }
+RT_DEV float ldf(const uint32_t* __restrict__ w, size_t i) { return __uint_as_float(__ldg(w + i)); }
+RT_DEV F3 ld3(const uint32_t* __restrict__ w, size_t i) { return {ldf(w, i), ldf(w, i + 1), ldf(w, i + 2)}; }
+RT_DEV uint4 ld4(const uint32_t* __restrict__ w, size_t i) {
+  return __ldg(reinterpret_cast<const uint4*>(w + i));
+}
+
+struct Ray {
+  F3 o;
+  float tmin;
+  F3 d;
+  float tmax;
+};
+RT_DEV Ray load_ray(const float4* __restrict__ rays, uint32_t i) {
+  float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+  return Ray{{a.x, a.y, a.z}, a.w, {b.x, b.y, b.z}, b.w};
+}
+
+// Device-side counters every traversal kernel may bump (rare events only).
+struct DevStatus {
+  unsigned long long stack_drops;
+  unsigned long long reserved[7];
+};
+
+}  // namespace rtk

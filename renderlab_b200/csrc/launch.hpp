@@ -1,0 +1,30 @@
+// Internal launcher interface between the C ABI (rt_api.cu) and the kernel translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+
+#include "kernels/common.cuh"
+
+namespace rtl {
+
+struct SceneView {
+  uint32_t layout;        // 0 GI, 1 reflection
+  const uint32_t* words;  // device words
+  size_t n_words;
+  uint32_t instances;
+  uint32_t top;
+  // Derived 8-wide layout for the WIDE8 kernel (null until built).
+  const void* wide8;
+  size_t wide8_bytes;
+};
+
+// PLAIN: mode 0 closest, 1/2 any-hit. Hits as documented in rt_trace.h.
+cudaError_t launch_plain(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
+                         rtk::DevStatus* st, cudaStream_t stream);
+// FAST: bit-exact with PLAIN; `order` (optional) permutes which ray each thread traces.
+cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
+                        uint32_t n, rtk::DevStatus* st, cudaStream_t stream);
+cudaError_t launch_selftest(uint32_t* out16, cudaStream_t stream);
+
+}  // namespace rtl

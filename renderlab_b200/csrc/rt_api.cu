@@ -1,0 +1,423 @@
+// The C ABI (include/rt_trace.h): contexts, scene upload, traversal dispatch, host builders.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <thread>
+#include <vector>
+
+#include "../../include/rt_trace.h"
+#include "host/host.hpp"
+#include "launch.hpp"
+
+struct rt_scene {
+  uint32_t layout = 0;
+  uint32_t* d_words = nullptr;
+  size_t n_words = 0;
+  rtb::SceneInfo info;
+  size_t device_bytes = 0;
+  void* d_wide8 = nullptr;
+  size_t wide8_bytes = 0;
+};
+
+struct rt_blas {
+  rtb::Blas b;
+};
+
+struct rt_ctx {
+  int device = 0;
+  rtk::DevStatus* d_status = nullptr;
+  uint32_t* d_scratch = nullptr;  // 16 words for the self-test
+  std::mutex mu;
+  std::string last_error;
+  std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
+  // rt_trace_host staging: two chunks in flight on two streams.
+  cudaStream_t streams[2] = {nullptr, nullptr};
+  void* d_rays = nullptr;
+  void* d_hits = nullptr;
+  size_t stage_rays = 0;  // rays per chunk buffer
+};
+
+namespace {
+
+constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BYTES = 32;
+constexpr uint32_t HOST_CHUNK = 1u << 20;
+
+rt_status fail(rt_ctx* ctx, rt_status s, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return s;
+}
+
+#define RT_CUDA(ctx, call)                                                                     \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+size_t hit_bytes(uint32_t layout, uint32_t mode) {
+  if (mode != 0) return ANY_HIT_BYTES;
+  return layout == 0 ? GI_HIT_BYTES : RS_HIT_BYTES;
+}
+
+rtl::SceneView view_of(const rt_scene* s) {
+  rtl::SceneView v;
+  v.layout = s->layout;
+  v.words = s->d_words;
+  v.n_words = s->n_words;
+  v.instances = s->info.instances;
+  v.top = s->info.top;
+  v.wide8 = s->d_wide8;
+  v.wide8_bytes = s->wide8_bytes;
+  return v;
+}
+
+rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* rays,
+                   const uint32_t* order, void* hits, uint32_t n, cudaStream_t stream) {
+  const rtl::SceneView v = view_of(scene);
+  const float4* r = reinterpret_cast<const float4*>(rays);
+  cudaError_t e;
+  switch (kernel) {
+    case RT_KERNEL_PLAIN:
+      if (order) return fail(ctx, RT_ERR_UNSUPPORTED, "the PLAIN kernel takes no ray order");
+      e = rtl::launch_plain(v, (uint32_t)mode, r, hits, n, ctx->d_status, stream);
+      break;
+    case RT_KERNEL_FAST:
+      e = rtl::launch_fast(v, (uint32_t)mode, r, order, hits, n, ctx->d_status, stream);
+      break;
+    default:
+      return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
+  }
+  if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "traversal launch: %s", cudaGetErrorString(e));
+  ctx->rays += n;
+  ctx->launches += 1;
+  return RT_OK;
+}
+
+rt_status check_trace_args(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel) {
+  if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null context or scene");
+  if ((unsigned)mode > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown mode %d", (int)mode);
+  if ((unsigned)kernel > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown kernel %d", (int)kernel);
+  return RT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t rt_abi_version(void) { return RT_ABI_VERSION; }
+
+rt_status rt_ctx_create(int device, rt_ctx** out) {
+  if (!out) return RT_ERR_INVALID_ARG;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || device < 0 || device >= count) return RT_ERR_CUDA;
+  auto ctx = std::make_unique<rt_ctx>();
+  ctx->device = device;
+  if (cudaSetDevice(device) != cudaSuccess) return RT_ERR_CUDA;
+  if (cudaMalloc(&ctx->d_status, sizeof(rtk::DevStatus)) != cudaSuccess) return RT_ERR_OOM;
+  if (cudaMemset(ctx->d_status, 0, sizeof(rtk::DevStatus)) != cudaSuccess) return RT_ERR_CUDA;
+  if (cudaMalloc(&ctx->d_scratch, 64) != cudaSuccess) return RT_ERR_OOM;
+  for (auto& s : ctx->streams)
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return RT_ERR_CUDA;
+  *out = ctx.release();
+  return RT_OK;
+}
+
+void rt_ctx_destroy(rt_ctx* ctx) {
+  if (!ctx) return;
+  cudaSetDevice(ctx->device);
+  for (auto s : ctx->streams)
+    if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
+  cudaFree(ctx->d_status);
+  cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_rays);
+  cudaFree(ctx->d_hits);
+  delete ctx;
+}
+
+const char* rt_get_last_error(const rt_ctx* ctx) { return ctx ? ctx->last_error.c_str() : "null context"; }
+
+rt_status rt_get_stats(rt_ctx* ctx, rt_stats* out) {
+  if (!ctx || !out) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  rtk::DevStatus st;
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, cudaMemcpy(&st, ctx->d_status, sizeof st, cudaMemcpyDeviceToHost));
+  out->rays_traced = ctx->rays;
+  out->stack_overflows = st.stack_drops;
+  out->launches = ctx->launches;
+  out->scene_bytes = ctx->scene_bytes;
+  return RT_OK;
+}
+
+rt_status rt_selftest(rt_ctx* ctx, uint32_t out[16]) {
+  if (!ctx || !out) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, rtl::launch_selftest(ctx->d_scratch, nullptr));
+  RT_CUDA(ctx, cudaMemcpy(out, ctx->d_scratch, 64, cudaMemcpyDeviceToHost));
+  return RT_OK;
+}
+
+rt_status rt_scene_upload(rt_ctx* ctx, rt_layout layout, const uint32_t* words, size_t n_words, rt_scene** out) {
+  if (!ctx || !words || !out) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  *out = nullptr;
+  if ((unsigned)layout > 1u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown layout %d", (int)layout);
+  auto s = std::make_unique<rt_scene>();
+  s->layout = (uint32_t)layout;
+  std::string err;
+  if (!rtb::validate_scene(s->layout, words, n_words, s->info, err))
+    return fail(ctx, RT_ERR_LAYOUT, "scene rejected: %s", err.c_str());
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t bytes = std::max<size_t>(n_words, 4) * 4;
+  if (cudaMalloc(&s->d_words, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RT_ERR_OOM, "device allocation of %zu bytes failed", bytes);
+  }
+  s->n_words = n_words;
+  s->device_bytes = bytes;
+  cudaError_t e = cudaMemcpy(s->d_words, words, n_words * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(s->d_words);
+    return fail(ctx, RT_ERR_CUDA, "scene copy: %s", cudaGetErrorString(e));
+  }
+  ctx->scene_bytes += s->device_bytes;
+  *out = s.release();
+  return RT_OK;
+}
+
+rt_status rt_scene_validate(rt_layout layout, const uint32_t* words, size_t n_words, uint32_t info[8], char* err,
+                            size_t err_len) {
+  if (!words || (unsigned)layout > 1u) return RT_ERR_INVALID_ARG;
+  rtb::SceneInfo si;
+  std::string e;
+  bool ok = rtb::validate_scene((uint32_t)layout, words, n_words, si, e);
+  if (info) {
+    info[0] = si.instances, info[1] = si.top, info[2] = si.root;
+    info[3] = (uint32_t)std::min<size_t>(si.triangles, UINT32_MAX), info[4] = (uint32_t)std::min<size_t>(si.nodes, UINT32_MAX);
+    info[5] = si.max_blas_depth, info[6] = si.max_top_depth, info[7] = 0;
+  }
+  if (!ok && err && err_len) std::snprintf(err, err_len, "%s", e.c_str());
+  return ok ? RT_OK : RT_ERR_LAYOUT;
+}
+
+rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* words, size_t n_words) {
+  if (!ctx || !scene || !words) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if (n_words > scene->n_words) return fail(ctx, RT_ERR_INVALID_ARG, "record words exceed the scene");
+  // Validate the whole buffer as it will be: the new leading words over the old mesh words.
+  std::vector<uint32_t> all(scene->n_words);
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, cudaMemcpy(all.data(), scene->d_words, scene->n_words * 4, cudaMemcpyDeviceToHost));
+  std::copy(words, words + n_words, all.begin());
+  rtb::SceneInfo info;
+  std::string err;
+  if (!rtb::validate_scene(scene->layout, all.data(), all.size(), info, err))
+    return fail(ctx, RT_ERR_LAYOUT, "records rejected: %s", err.c_str());
+  RT_CUDA(ctx, cudaMemcpy(scene->d_words, words, n_words * 4, cudaMemcpyHostToDevice));
+  scene->info = info;
+  return RT_OK;
+}
+
+rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene) {
+  if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  cudaSetDevice(ctx->device);
+  cudaFree(scene->d_words);
+  cudaFree(scene->d_wide8);
+  ctx->scene_bytes -= scene->device_bytes;
+  delete scene;
+  return RT_OK;
+}
+
+size_t rt_scene_device_bytes(const rt_scene* scene) { return scene ? scene->device_bytes : 0; }
+
+rt_status rt_trace(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, const rt_ray* d_rays, void* d_hits, uint32_t n,
+                   void* stream) {
+  return rt_trace_ex(ctx, scene, mode, RT_KERNEL_PLAIN, d_rays, nullptr, d_hits, n, stream);
+}
+
+rt_status rt_trace_ex(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* d_rays,
+                      const uint32_t* d_order, void* d_hits, uint32_t n, void* stream) {
+  rt_status s = check_trace_args(ctx, scene, mode, kernel);
+  if (s != RT_OK) return s;
+  if (n == 0) return RT_OK;
+  if (!d_rays || !d_hits) return fail(ctx, RT_ERR_INVALID_ARG, "null ray or hit buffer");
+  if (reinterpret_cast<uintptr_t>(d_rays) % 16 != 0) return fail(ctx, RT_ERR_INVALID_ARG, "rays must be 16-byte aligned");
+  if (reinterpret_cast<uintptr_t>(d_hits) % 4 != 0) return fail(ctx, RT_ERR_INVALID_ARG, "hits must be 4-byte aligned");
+  return dispatch(ctx, scene, mode, kernel, d_rays, d_order, d_hits, n, static_cast<cudaStream_t>(stream));
+}
+
+rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays) {
+  if (!ctx) return RT_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  const size_t want = std::min<size_t>(max_rays, HOST_CHUNK);
+  if (want <= ctx->stage_rays) return RT_OK;
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  for (auto s : ctx->streams) RT_CUDA(ctx, cudaStreamSynchronize(s));
+  cudaFree(ctx->d_rays);
+  cudaFree(ctx->d_hits);
+  ctx->d_rays = ctx->d_hits = nullptr;
+  ctx->stage_rays = 0;
+  if (cudaMalloc(&ctx->d_rays, 2 * want * RAY_BYTES) != cudaSuccess ||
+      cudaMalloc(&ctx->d_hits, 2 * want * GI_HIT_BYTES) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RT_ERR_OOM, "staging allocation for %zu rays failed", want);
+  }
+  ctx->stage_rays = want;
+  return RT_OK;
+}
+
+rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* h_rays,
+                        void* h_hits, uint32_t n) {
+  rt_status s = check_trace_args(ctx, scene, mode, kernel);
+  if (s != RT_OK) return s;
+  if (n == 0) return RT_OK;
+  if (!h_rays || !h_hits) return fail(ctx, RT_ERR_INVALID_ARG, "null ray or hit buffer");
+  if ((s = rt_ctx_reserve(ctx, n)) != RT_OK) return s;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const size_t hb = hit_bytes(scene->layout, (uint32_t)mode);
+  const uint32_t chunk = (uint32_t)ctx->stage_rays;
+  for (uint32_t off = 0, c = 0; off < n; off += chunk, ++c) {
+    const uint32_t m = std::min(chunk, n - off);
+    const int b = c & 1;
+    cudaStream_t st = ctx->streams[b];
+    char* dr = static_cast<char*>(ctx->d_rays) + (size_t)b * chunk * RAY_BYTES;
+    char* dh = static_cast<char*>(ctx->d_hits) + (size_t)b * chunk * GI_HIT_BYTES;
+    RT_CUDA(ctx, cudaMemcpyAsync(dr, h_rays + off, (size_t)m * RAY_BYTES, cudaMemcpyHostToDevice, st));
+    rt_status d = dispatch(ctx, scene, mode, kernel, reinterpret_cast<const rt_ray*>(dr), nullptr, dh, m, st);
+    if (d != RT_OK) return d;
+    RT_CUDA(ctx, cudaMemcpyAsync(static_cast<char*>(h_hits) + (size_t)off * hb, dh, (size_t)m * hb,
+                                 cudaMemcpyDeviceToHost, st));
+  }
+  for (auto st : ctx->streams) RT_CUDA(ctx, cudaStreamSynchronize(st));
+  return RT_OK;
+}
+
+// ---------------------------------------------------------------- host builders
+
+rt_status rt_blas_build(const float* positions, uint32_t n_positions, const uint32_t* indices, uint32_t n_indices,
+                        uint32_t build_flags, rt_blas** out) {
+  if (!positions || !indices || !out) return RT_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto b = std::make_unique<rt_blas>();
+  std::string err;
+  bool ok = (build_flags & RT_BUILD_MEDIAN)
+                ? rtb::build_blas(positions, n_positions, indices, n_indices, false, b->b, err)
+                : rtb::build_blas_sah(positions, n_positions, indices, n_indices, b->b, err);
+  if (!ok) return RT_ERR_INVALID_ARG;
+  *out = b.release();
+  return RT_OK;
+}
+
+rt_status rt_blas_info(const rt_blas* blas, uint32_t info[6]) {
+  if (!blas || !info) return RT_ERR_INVALID_ARG;
+  const rtb::Blas& b = blas->b;
+  info[0] = (uint32_t)b.node_count();
+  info[1] = (uint32_t)b.leaf_count();
+  info[2] = (uint32_t)(b.positions.size() / 3);
+  info[3] = (uint32_t)b.indices.size();
+  info[4] = b.root;
+  info[5] = (uint32_t)rtb::blas_depth(b, b.root);
+  return RT_OK;
+}
+
+rt_status rt_blas_nodes(const rt_blas* blas, uint32_t* out) {
+  if (!blas || !out) return RT_ERR_INVALID_ARG;
+  std::copy(blas->b.nodes.begin(), blas->b.nodes.end(), out);
+  return RT_OK;
+}
+
+rt_status rt_blas_indices(const rt_blas* blas, uint32_t* out) {
+  if (!blas || !out) return RT_ERR_INVALID_ARG;
+  std::copy(blas->b.indices.begin(), blas->b.indices.end(), out);
+  return RT_OK;
+}
+
+rt_status rt_blas_refit(rt_blas* blas, const float* positions, uint32_t n_positions) {
+  if (!blas || !positions) return RT_ERR_INVALID_ARG;
+  std::string err;
+  return rtb::refit_blas(blas->b, positions, n_positions, err) ? RT_OK : RT_ERR_INVALID_ARG;
+}
+
+void rt_blas_free(rt_blas* blas) { delete blas; }
+
+rt_status rt_pack_scene(rt_layout layout, const rt_blas* const* meshes, uint32_t n_meshes,
+                        const float* const* mesh_positions, const uint32_t* const* mesh_indices,
+                        const uint32_t* mesh_n_indices, const uint32_t* mesh_primitives, const rt_instance* instances,
+                        uint32_t n_instances, int tlas_mode, uint32_t* out_words, size_t* n_words) {
+  if (!n_words || (n_meshes && (!meshes || !mesh_positions || !mesh_indices || !mesh_n_indices)) ||
+      (n_instances && !instances))
+    return RT_ERR_INVALID_ARG;
+  std::vector<rtb::MeshRef> refs(n_meshes);
+  for (uint32_t m = 0; m < n_meshes; ++m) {
+    if (!meshes[m]) return RT_ERR_INVALID_ARG;
+    refs[m] = rtb::MeshRef{&meshes[m]->b, mesh_positions[m], mesh_indices[m], mesh_n_indices[m],
+                           mesh_primitives ? mesh_primitives[m] != 0 : false};
+  }
+  std::vector<rtb::Placement> inst(n_instances);
+  for (uint32_t i = 0; i < n_instances; ++i) {
+    const rt_instance& s = instances[i];
+    rtb::Placement& p = inst[i];
+    std::copy(s.model, s.model + 12, p.model);
+    std::copy(s.rows, s.rows + 12, p.rows);
+    p.mesh = s.mesh, p.slot = s.slot, p.casts_shadow = s.casts_shadow, p.near_base = s.near_base;
+    std::copy(s.extra, s.extra + 8, p.extra);
+  }
+  std::vector<uint32_t> words;
+  std::string err;
+  bool ok = layout == RT_LAYOUT_GI ? rtb::pack_gi(refs, inst, tlas_mode, words, err)
+                                   : rtb::pack_reflection(refs, inst, tlas_mode, words, err);
+  if (!ok) return RT_ERR_LAYOUT;
+  if (!out_words) {
+    *n_words = words.size();
+    return RT_OK;
+  }
+  if (*n_words < words.size()) {
+    *n_words = words.size();
+    return RT_ERR_INVALID_ARG;
+  }
+  std::copy(words.begin(), words.end(), out_words);
+  *n_words = words.size();
+  return RT_OK;
+}
+
+rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words) {
+  if (!boxes || !n_words || n < 2) return RT_ERR_INVALID_ARG;
+  std::vector<rtb::Aabb> b(n);
+  for (uint32_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) b[i].lo[a] = boxes[6 * i + a], b[i].hi[a] = boxes[6 * i + 3 + a];
+  std::vector<uint32_t> nodes = rtb::tlas_build(b, sah != 0);
+  if (!out) {
+    *n_words = nodes.size();
+    return RT_OK;
+  }
+  if (*n_words < nodes.size()) {
+    *n_words = nodes.size();
+    return RT_ERR_INVALID_ARG;
+  }
+  std::copy(nodes.begin(), nodes.end(), out);
+  *n_words = nodes.size();
+  return RT_OK;
+}
+
+rt_status rt_tlas_refit(uint32_t* nodes, size_t n_words, const float* boxes, uint32_t n) {
+  if (!nodes || !boxes || n < 2 || n_words < 32) return RT_ERR_INVALID_ARG;
+  std::vector<rtb::Aabb> b(n);
+  for (uint32_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) b[i].lo[a] = boxes[6 * i + a], b[i].hi[a] = boxes[6 * i + 3 + a];
+  rtb::tlas_refit(nodes, b);
+  return RT_OK;
+}
+
+}  // extern "C"
