@@ -125,6 +125,9 @@ rt_status rt_scene_validate(rt_layout layout, const uint32_t* words, size_t n_wo
                             char* err, size_t err_len);
 rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* words,
                                   size_t n_words);
+/* Builds the derived layout a kernel needs (RT_KERNEL_WIDE8: the compressed 8-wide BVH over the
+ * scene's triangles, built on the host threads and uploaded). PLAIN and FAST need nothing. */
+rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel);
 rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene);
 size_t rt_scene_device_bytes(const rt_scene* scene);
 

@@ -83,6 +83,10 @@ void blas64(const uint32_t* w, size_t nodes, uint32_t root, D3 o, D3 d, double t
         uint8_t ql = (w[n + 10 + a] >> (8 * s)) & 255u, qh = (w[n + 13 + a] >> (8 * s)) & 255u;
         lo[a] = (double)(org[a] + stp[a] * (float)ql);  // cluster_bvh.rs:45 unfused decode
         hi[a] = (double)(org[a] + stp[a] * (float)qh);
+        // Widened by 1e-9 relative: the f64 slab test then never culls a hit the f64 triangle
+        // test accepts (a ray grazing a box face), so the walk equals a brute force.
+        lo[a] -= 1e-9 * (std::fabs(lo[a]) + 1.0);
+        hi[a] += 1e-9 * (std::fabs(hi[a]) + 1.0);
       }
       double lim = best.hit ? best.t : tmax;
       if (box_hit(o, d, tmin, lo, hi, lim)) stack.push_back(c);
@@ -103,7 +107,11 @@ inline void rows64(const uint32_t* w, size_t r, const Ray& ray, D3& o, D3& d) {
 
 inline bool world_box(const uint32_t* w, size_t r, const Ray& ray, double tmin, double lim) {
   double lo[3], hi[3];
-  for (int a = 0; a < 3; ++a) lo[a] = bitsf(w[r + 12 + a]), hi[a] = bitsf(w[r + 15 + a]);
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = bitsf(w[r + 12 + a]), hi[a] = bitsf(w[r + 15 + a]);
+    lo[a] -= 1e-9 * (std::fabs(lo[a]) + 1.0);
+    hi[a] += 1e-9 * (std::fabs(hi[a]) + 1.0);
+  }
   D3 o = {ray.o[0], ray.o[1], ray.o[2]}, d = {ray.d[0], ray.d[1], ray.d[2]};
   return box_hit(o, d, tmin, lo, hi, lim);
 }

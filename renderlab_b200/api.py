@@ -56,7 +56,7 @@ class RtInstance(ctypes.Structure):
 
 EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
-           "rt_scene_device_bytes", "rt_scene_validate", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve",
+           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve",
            "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
 
@@ -84,6 +84,7 @@ def lib() -> ctypes.CDLL:
     L.rt_scene_validate.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, _u32p, ctypes.c_char_p, ctypes.c_size_t]
     L.rt_scene_update_records.argtypes = [_vp, _vp, _u32p, ctypes.c_size_t]
     L.rt_scene_release.argtypes = [_vp, _vp]
+    L.rt_scene_prepare.argtypes = [_vp, _vp, ctypes.c_int]
     L.rt_scene_device_bytes.argtypes = [_vp]
     L.rt_scene_device_bytes.restype = ctypes.c_size_t
     L.rt_trace.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
@@ -254,6 +255,10 @@ class Scene:
         if self.handle:
             self.engine._check(lib().rt_scene_release(self.engine.ctx, self.handle))
             self.handle = None
+
+    def prepare(self, kernel: str = "wide8"):
+        """Build the derived layout `kernel` reads (the 8-wide BVH for "wide8")."""
+        self.engine._check(lib().rt_scene_prepare(self.engine.ctx, self.handle, KERNELS[kernel]))
 
     def update_records(self, words):
         w = np.ascontiguousarray(words, np.uint32)

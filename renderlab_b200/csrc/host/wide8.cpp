@@ -1,0 +1,387 @@
+// Builder of the compressed 8-wide BLAS (layout in wide8.hpp): a binned-SAH binary tree with
+// leaves of at most three triangles, collapsed top-down into 8-wide nodes by repeatedly opening
+// the child of largest surface area, child slots assigned by octant, child boxes quantised
+// outward to 8 bits against a power-of-two scale.
+#include "wide8.hpp"
+
+#include <algorithm>
+#include <atomic>
+#include <cfloat>
+#include <cmath>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <numeric>
+#include <thread>
+
+#include "host.hpp"
+
+namespace rtb {
+
+namespace {
+
+constexpr int BINS = 32;
+constexpr float COST_NODE = 1.0f, COST_TRI = 1.0f;
+
+double area(const Aabb& b) {
+  double e0 = std::max(0.0, (double)b.hi[0] - b.lo[0]), e1 = std::max(0.0, (double)b.hi[1] - b.lo[1]),
+         e2 = std::max(0.0, (double)b.hi[2] - b.lo[2]);
+  return e0 * e1 + e1 * e2 + e2 * e0;
+}
+
+struct BNode {
+  Aabb box;
+  int kid[2];
+  uint32_t first, count;  // count > 0: leaf over refs[first, first + count)
+};
+
+class Binary {
+ public:
+  explicit Binary(const std::vector<SrcTri>& t) : tris_(t) {
+    const size_t n = t.size();
+    box_.resize(n);
+    cen_.resize(3 * n);
+    for (size_t i = 0; i < n; ++i) {
+      Aabb b = Aabb::empty();
+      for (int k = 0; k < 3; ++k) b.grow(&t[i].v[3 * k]);
+      box_[i] = b;
+      for (int a = 0; a < 3; ++a) cen_[3 * i + a] = 0.5f * (b.lo[a] + b.hi[a]);
+    }
+    ref_.resize(n);
+    std::iota(ref_.begin(), ref_.end(), 0u);
+  }
+  int build() { return node(0, (uint32_t)ref_.size()); }
+  const std::vector<BNode>& nodes() const { return nodes_; }
+  const std::vector<uint32_t>& refs() const { return ref_; }
+
+ private:
+  const std::vector<SrcTri>& tris_;
+  std::vector<Aabb> box_;
+  std::vector<float> cen_;
+  std::vector<uint32_t> ref_;
+  std::vector<BNode> nodes_;
+
+  int leaf(uint32_t first, uint32_t n, const Aabb& b) {
+    nodes_.push_back(BNode{b, {-1, -1}, first, n});
+    return (int)nodes_.size() - 1;
+  }
+
+  int node(uint32_t first, uint32_t n) {
+    Aabb b = Aabb::empty(), cb = Aabb::empty();
+    for (uint32_t k = first; k < first + n; ++k) {
+      b.grow(box_[ref_[k]]);
+      cb.grow(&cen_[3 * (size_t)ref_[k]]);
+    }
+    if (n == 1) return leaf(first, n, b);
+    // binned SAH over the centroid bounds, all three axes
+    double best = INFINITY;
+    int best_axis = -1, best_bin = 0;
+    const double parent = std::max(area(b), 1e-30);
+    for (int a = 0; a < 3; ++a) {
+      const float ext = cb.hi[a] - cb.lo[a];
+      if (!(ext > 0.0f)) continue;
+      const float scale = (float)BINS / ext;
+      uint32_t cnt[BINS] = {};
+      Aabb bb[BINS];
+      for (auto& x : bb) x = Aabb::empty();
+      for (uint32_t k = first; k < first + n; ++k) {
+        uint32_t r = ref_[k];
+        int bin = std::min(BINS - 1, (int)((cen_[3 * (size_t)r + a] - cb.lo[a]) * scale));
+        cnt[bin]++;
+        bb[bin].grow(box_[r]);
+      }
+      double ra[BINS];
+      uint32_t rn[BINS];
+      Aabb acc = Aabb::empty();
+      uint32_t m = 0;
+      for (int k = BINS - 1; k > 0; --k) {
+        acc.grow(bb[k]);
+        m += cnt[k];
+        ra[k] = area(acc);
+        rn[k] = m;
+      }
+      acc = Aabb::empty();
+      m = 0;
+      for (int k = 0; k < BINS - 1; ++k) {
+        acc.grow(bb[k]);
+        m += cnt[k];
+        if (m == 0 || rn[k + 1] == 0) continue;
+        double c = COST_NODE + COST_TRI * (area(acc) * m + ra[k + 1] * rn[k + 1]) / parent;
+        if (c < best) best = c, best_axis = a, best_bin = k;
+      }
+    }
+    if (n <= W8_MAX_LEAF && (best_axis < 0 || COST_TRI * n <= best)) return leaf(first, n, b);
+    uint32_t mid;
+    if (best_axis >= 0) {
+      const float ext = cb.hi[best_axis] - cb.lo[best_axis], scale = (float)BINS / ext, lo = cb.lo[best_axis];
+      auto it = std::partition(ref_.begin() + first, ref_.begin() + first + n, [&](uint32_t r) {
+        return std::min(BINS - 1, (int)((cen_[3 * (size_t)r + best_axis] - lo) * scale)) <= best_bin;
+      });
+      mid = (uint32_t)(it - ref_.begin());
+    } else {
+      mid = first + n / 2;  // coincident centroids: split the list
+    }
+    const int me = (int)nodes_.size();
+    nodes_.push_back(BNode{b, {-1, -1}, 0, 0});
+    const int l = node(first, mid - first);
+    const int r = node(mid, first + n - mid);
+    nodes_[me].kid[0] = l;
+    nodes_[me].kid[1] = r;
+    return me;
+  }
+};
+
+// Smallest power-of-two exponent e with 255 * 2^e >= ext (a normal float scale).
+int scale_exponent(double ext) {
+  if (!(ext > 0.0)) return -126;
+  int e;
+  std::frexp(ext / 255.0, &e);  // ext/255 = f * 2^e, f in [0.5, 1)
+  while (std::ldexp(255.0, e - 1) >= ext && e - 1 >= -126) --e;
+  while (std::ldexp(255.0, e) < ext) ++e;
+  return std::max(-126, std::min(127, e));
+}
+
+}  // namespace
+
+void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
+  out = Wide8Blas{};
+  if (tris.empty()) return;
+  Binary bin(tris);
+  const int broot = bin.build();
+  const auto& bn = bin.nodes();
+  const auto& refs = bin.refs();
+  struct Task { uint32_t wide; int b; };
+  std::deque<Task> queue;
+  out.nodes.resize(W8_NODE_WORDS, 0);
+  queue.push_back({0, broot});
+  while (!queue.empty()) {
+    const Task task = queue.front();
+    queue.pop_front();
+    std::vector<int> kids;
+    if (bn[task.b].count > 0) kids.push_back(task.b);
+    else kids = {bn[task.b].kid[0], bn[task.b].kid[1]};
+    while (kids.size() < 8) {
+      int pick = -1;
+      double pa = -1.0;
+      for (size_t k = 0; k < kids.size(); ++k)
+        if (bn[kids[k]].count == 0 && area(bn[kids[k]].box) > pa) pa = area(bn[kids[k]].box), pick = (int)k;
+      if (pick < 0) break;
+      const int b = kids[pick];
+      kids[pick] = bn[b].kid[0];
+      kids.insert(kids.begin() + pick + 1, bn[b].kid[1]);
+    }
+    // octant slots: greedy on the children's centre offsets from the node centre
+    Aabb nb = Aabb::empty();
+    for (int k : kids) nb.grow(bn[k].box);
+    double c0[3];
+    for (int a = 0; a < 3; ++a) c0[a] = 0.5 * ((double)nb.lo[a] + nb.hi[a]);
+    int slot_of[8];
+    std::fill(slot_of, slot_of + 8, -1);
+    {
+      double score[8][8];
+      for (size_t k = 0; k < kids.size(); ++k)
+        for (int s = 0; s < 8; ++s) {
+          double v = 0;
+          for (int a = 0; a < 3; ++a) {
+            double c = 0.5 * ((double)bn[kids[k]].box.lo[a] + bn[kids[k]].box.hi[a]) - c0[a];
+            v += (s >> a & 1) ? c : -c;
+          }
+          score[k][s] = v;
+        }
+      bool kid_done[8] = {}, slot_done[8] = {};
+      for (size_t round = 0; round < kids.size(); ++round) {
+        double bs = -INFINITY;
+        int bk = -1, bsl = -1;
+        for (size_t k = 0; k < kids.size(); ++k)
+          if (!kid_done[k])
+            for (int s = 0; s < 8; ++s)
+              if (!slot_done[s] && score[k][s] > bs) bs = score[k][s], bk = (int)k, bsl = s;
+        kid_done[bk] = slot_done[bsl] = true;
+        slot_of[bsl] = bk;
+      }
+    }
+    uint32_t* w = &out.nodes[(size_t)task.wide * W8_NODE_WORDS];
+    // scale
+    float p[3];
+    int ex[3];
+    for (int a = 0; a < 3; ++a) {
+      p[a] = nb.lo[a];
+      ex[a] = scale_exponent((double)nb.hi[a] - (double)p[a]);
+    }
+    uint32_t imask = 0, child_base = (uint32_t)(out.nodes.size() / W8_NODE_WORDS),
+             tri_base = (uint32_t)(out.tris.size() / W8_TRI_WORDS);
+    uint8_t meta[8] = {}, q[6][8] = {};
+    uint32_t inner = 0, offset = 0;
+    for (int s = 0; s < 8; ++s) {
+      if (slot_of[s] < 0) continue;
+      const BNode& k = bn[kids[slot_of[s]]];
+      for (int a = 0; a < 3; ++a) {
+        const double sc = std::ldexp(1.0, ex[a]);
+        double lo = std::floor(((double)k.box.lo[a] - p[a]) / sc), hi = std::ceil(((double)k.box.hi[a] - p[a]) / sc);
+        q[a][s] = (uint8_t)std::max(0.0, std::min(255.0, lo));
+        q[3 + a][s] = (uint8_t)std::max(0.0, std::min(255.0, hi));
+      }
+      if (k.count == 0) {
+        imask |= 1u << s;
+        ++inner;
+      } else {
+        meta[s] = (uint8_t)(k.count << 5 | offset);
+        for (uint32_t t = 0; t < k.count; ++t) {
+          const SrcTri& src = tris[refs[k.first + t]];
+          for (int j = 0; j < 9; ++j) out.tris.push_back(as_bits(src.v[j]));
+          out.tris.push_back(src.ident);
+          out.tris.push_back(src.ref);
+          out.tris.push_back(0);
+        }
+        offset += k.count;
+      }
+    }
+    out.nodes.resize(out.nodes.size() + (size_t)inner * W8_NODE_WORDS, 0);
+    w = &out.nodes[(size_t)task.wide * W8_NODE_WORDS];
+    for (int a = 0; a < 3; ++a) w[a] = as_bits(p[a]);
+    w[3] = (uint32_t)(ex[0] + 127) | (uint32_t)(ex[1] + 127) << 8 | (uint32_t)(ex[2] + 127) << 16 | imask << 24;
+    w[4] = child_base;
+    w[5] = tri_base;
+    w[6] = meta[0] | meta[1] << 8 | meta[2] << 16 | (uint32_t)meta[3] << 24;
+    w[7] = meta[4] | meta[5] << 8 | meta[6] << 16 | (uint32_t)meta[7] << 24;
+    for (int plane = 0; plane < 6; ++plane) {
+      w[8 + 2 * plane] = q[plane][0] | q[plane][1] << 8 | q[plane][2] << 16 | (uint32_t)q[plane][3] << 24;
+      w[9 + 2 * plane] = q[plane][4] | q[plane][5] << 8 | q[plane][6] << 16 | (uint32_t)q[plane][7] << 24;
+    }
+    uint32_t next = child_base;
+    for (int s = 0; s < 8; ++s)
+      if (slot_of[s] >= 0 && bn[kids[slot_of[s]]].count == 0) queue.push_back({next++, kids[slot_of[s]]});
+  }
+}
+
+namespace {
+
+// Triangles of one BLAS of the packed words, in the BVH4-Q8's leaf order.
+void gather(uint32_t layout, const uint32_t* w, const uint32_t* rec, std::vector<SrcTri>& out) {
+  std::vector<uint32_t> stack;
+  if (layout == 1) {
+    const size_t nodes = rec[18] & ~3u, tris = rec[19] & ~3u;
+    stack.push_back(rec[20]);
+    while (!stack.empty()) {
+      uint32_t c = stack.back();
+      stack.pop_back();
+      if (c & LEAF) {
+        const uint32_t start = (c & ~LEAF) >> 4, cnt = c & 15u;
+        for (uint32_t k = 0; k < cnt; ++k) {
+          const size_t X = tris + 12 * (size_t)(start + k);
+          SrcTri t;
+          for (int a = 0; a < 3; ++a) {
+            const double va = as_float(w[X + a]);
+            t.v[a] = (float)va;
+            t.v[3 + a] = (float)(va + (double)as_float(w[X + 3 + a]));
+            t.v[6 + a] = (float)(va + (double)as_float(w[X + 6 + a]));
+          }
+          t.ident = w[X + 9];
+          t.ref = (uint32_t)X;
+          out.push_back(t);
+        }
+        continue;
+      }
+      const uint32_t* n = w + nodes + 16 * (size_t)c;
+      for (int s = 3; s >= 0; --s)
+        if (n[6 + s] != EMPTY) stack.push_back(n[6 + s]);
+    }
+    return;
+  }
+  const size_t nodes = rec[18], leaves = rec[19], positions = rec[20], indices = rec[21];
+  stack.push_back(rec[22]);
+  while (!stack.empty()) {
+    uint32_t c = stack.back();
+    stack.pop_back();
+    if (c & LEAF) {
+      const size_t l = leaves + 2 * (size_t)(c & ~LEAF);
+      const uint32_t first = w[l], cnt = w[l + 1];
+      for (uint32_t k = 0; k < cnt; k += 3) {
+        const size_t x = indices + first + k;
+        SrcTri t;
+        for (int j = 0; j < 3; ++j)
+          for (int a = 0; a < 3; ++a) t.v[3 * j + a] = as_float(w[positions + 3 * (size_t)w[x + j] + a]);
+        t.ident = (first + k) / 3;
+        t.ref = (uint32_t)x;
+        out.push_back(t);
+      }
+      continue;
+    }
+    const uint32_t* n = w + nodes + 16 * (size_t)c;
+    for (int s = 3; s >= 0; --s)
+      if (n[6 + s] != EMPTY) stack.push_back(n[6 + s]);
+  }
+}
+
+}  // namespace
+
+bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8Scene& out, std::string& err,
+                       int threads) {
+  (void)n_words;
+  out = Wide8Scene{};
+  const uint32_t count = w[0];
+  const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
+  std::map<std::vector<uint32_t>, uint32_t> key_to_blas;
+  std::vector<const uint32_t*> first_rec;
+  std::vector<uint32_t> blas_of(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint32_t* r = w + header + stride * (size_t)i;
+    std::vector<uint32_t> key = layout == 0 ? std::vector<uint32_t>{r[18], r[19], r[20], r[21], r[22]}
+                                            : std::vector<uint32_t>{r[18] & ~3u, r[19] & ~3u, r[20]};
+    auto it = key_to_blas.find(key);
+    if (it == key_to_blas.end()) {
+      it = key_to_blas.emplace(key, (uint32_t)first_rec.size()).first;
+      first_rec.push_back(r);
+    }
+    blas_of[i] = it->second;
+  }
+  const size_t nb = first_rec.size();
+  std::vector<Wide8Blas> built(nb);
+  std::atomic<size_t> next{0};
+  auto work = [&] {
+    for (;;) {
+      size_t b = next.fetch_add(1);
+      if (b >= nb) break;
+      std::vector<SrcTri> tris;
+      gather(layout, w, first_rec[b], tris);
+      build_wide8(tris, built[b]);
+    }
+  };
+  const int nt = std::max(1, std::min<int>(threads, (int)nb));
+  std::vector<std::thread> pool;
+  for (int t = 1; t < nt; ++t) pool.emplace_back(work);
+  work();
+  for (auto& t : pool) t.join();
+  std::vector<uint32_t> node_base(nb), tri_base(nb);
+  size_t nn = 0, ntri = 0;
+  for (size_t b = 0; b < nb; ++b) {
+    node_base[b] = (uint32_t)nn;
+    tri_base[b] = (uint32_t)ntri;
+    nn += built[b].nodes.size() / W8_NODE_WORDS;
+    ntri += built[b].tris.size() / W8_TRI_WORDS;
+  }
+  if (nn >= (1u << 31) || ntri >= (1u << 31)) {
+    err = "8-wide layout too large";
+    return false;
+  }
+  out.nodes.reserve(nn * W8_NODE_WORDS);
+  out.tris.reserve(ntri * W8_TRI_WORDS);
+  for (size_t b = 0; b < nb; ++b) {
+    const size_t at = out.nodes.size();
+    out.nodes.insert(out.nodes.end(), built[b].nodes.begin(), built[b].nodes.end());
+    for (size_t k = at; k < out.nodes.size(); k += W8_NODE_WORDS) {
+      out.nodes[k + 4] += node_base[b];
+      out.nodes[k + 5] += tri_base[b];
+    }
+    out.tris.insert(out.tris.end(), built[b].tris.begin(), built[b].tris.end());
+  }
+  out.inst.resize(2 * (size_t)count);
+  for (uint32_t i = 0; i < count; ++i) {
+    out.inst[2 * i] = built[blas_of[i]].nodes.empty() ? EMPTY : node_base[blas_of[i]];
+    out.inst[2 * i + 1] = tri_base[blas_of[i]];
+  }
+  out.blas_count = nb;
+  return true;
+}
+
+}  // namespace rtb

@@ -1,0 +1,56 @@
+// The engine's compressed 8-wide BLAS (the WIDE8 kernel's layout), derived from an uploaded
+// scene's packed words.
+//
+// Node, 80 bytes (20 words, five 16-byte loads):
+//   0-2   p: float origin of the child boxes
+//   3     exponent bytes ex | ey << 8 | ez << 16 (scale 2^(e-127)), inner-child mask << 24
+//   4     index of the first inner child node (inner children are contiguous, in slot order)
+//   5     index of the first triangle (leaf children's triangles are contiguous, in slot order)
+//   6-7   meta byte per slot: leaf (count << 5 | offset), 0 for an inner or empty slot
+//   8-19  child boxes: lo x, lo y, lo z, hi x, hi y, hi z, one byte per slot (two words each)
+// A child box is the real interval [p + q_lo * 2^e, p + q_hi * 2^e] per axis; the builder
+// rounds q outward in exact arithmetic, so it encloses the child's triangles exactly.
+// Slots are assigned by octant: slot bit a set means the child lies toward +a, so a ray with
+// direction-sign bits o meets slot k ^ o roughly k-th (Ylitie, Karras, Laine 2017, "Efficient
+// Incoherent Ray Traversal on GPUs Through Compressed Wide BVHs").
+//
+// Triangle, 48 bytes (12 words): v0 xyz, v1 xyz, v2 xyz (f32, as the watertight test reads
+// them), ident (reflection: primitive id; GI: triangle ordinal in the mesh's index array), ref
+// (the word offset of the source triangle in the packed buffer: reflection a/e1/e2, GI its three
+// indices), 0.
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+namespace rtb {
+
+constexpr uint32_t W8_NODE_WORDS = 20;
+constexpr uint32_t W8_TRI_WORDS = 12;
+constexpr uint32_t W8_MAX_LEAF = 3;
+
+struct Wide8Blas {
+  std::vector<uint32_t> nodes;  // root is node 0
+  std::vector<uint32_t> tris;
+};
+
+// The whole derived scene: per distinct BLAS of the packed words, its nodes and triangles, and
+// per instance the (node base, triangle base) of its BLAS in the concatenated arrays.
+struct Wide8Scene {
+  std::vector<uint32_t> nodes;
+  std::vector<uint32_t> tris;
+  std::vector<uint32_t> inst;  // 2 words per instance: node base, triangle base
+  size_t blas_count = 0;
+};
+
+// Source triangle for the builder: f32 vertices plus identity words.
+struct SrcTri {
+  float v[9];
+  uint32_t ident, ref;
+};
+
+void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out);
+bool build_wide8_scene(uint32_t layout, const uint32_t* words, size_t n_words, Wide8Scene& out, std::string& err,
+                       int threads);
+
+}  // namespace rtb

@@ -1,0 +1,507 @@
+// WIDE8 traversal: the precision variant over the compressed 8-wide BLAS of host/wide8.hpp.
+//
+// * Top level and instance records: the packed words, walked as the reference does.
+// * BLAS: 80-byte nodes; a ray's direction-sign octant o orders the children (slot k ^ o is
+//   visited k-th); inner hits form a node group (first child, pending bits, inner mask) that is
+//   pushed whole, so the stack holds one entry per level.
+// * Child boxes: t = fma(q, 2^e / d, (p - o) / d) per plane, widened by a per-node bound on its
+//   rounding error so that no box a ray meets is ever culled (the boxes themselves enclose their
+//   triangles exactly).
+// * Triangles: the watertight test of Woop, Benthin and Wald (2013) through a per-instance
+//   shear matrix; an edge function that rounds to zero is recomputed in double. Shared vertices
+//   transform identically, so a ray never slips between two triangles.
+// * FP64: candidates whose f32 result is uncertain -- within 8e-6 relative of the current best
+//   (a near tie), of tmin or tmax, or within 1e-5 of an edge -- are re-intersected with the f64
+//   Möller-Trumbore test over the source triangle in the packed words, in the exact arithmetic
+//   of the f64 reference (crates/asset/src/cluster_bvh/reference.rs:121-158), and ties resolve
+//   on (t, instance, triangle) as it does.
+#pragma once
+#include "plain.cuh"
+
+namespace rtk {
+
+constexpr float W8_U = 5.9604645e-8f;  // 2^-24
+constexpr float W8_TIE = 8e-6f;
+constexpr float W8_EDGE = 1e-5f;
+constexpr uint32_t W8_STACK = 32;
+
+struct W8View {
+  const uint4* nodes;     // 5 uint4 a node
+  const uint4* tris;      // 3 uint4 a triangle
+  const uint32_t* inst;   // 2 words an instance: node base, triangle base
+};
+
+struct W8Best {
+  float t;          // f32 t of the best candidate (f32(t64) once re-tested)
+  float band;       // bound on |t - t64| while !has64
+  float abs_err;    // its absolute (coordinate-rounding) part
+  double t64;       // valid when has64
+  bool has64;
+  bool hit;
+  uint32_t inst;    // instance index
+  uint32_t tri;     // 8-wide triangle index
+  uint32_t ident;   // primitive id (reflection) or triangle ordinal (GI)
+  float u, v;
+};
+
+// f64 reference arithmetic, never contracted (reference.rs:47-59).
+struct D3 {
+  double x, y, z;
+};
+RT_DEV D3 dsub3(D3 a, D3 b) { return {__dsub_rn(a.x, b.x), __dsub_rn(a.y, b.y), __dsub_rn(a.z, b.z)}; }
+RT_DEV double ddot(D3 a, D3 b) { return __dadd_rn(__dadd_rn(__dmul_rn(a.x, b.x), __dmul_rn(a.y, b.y)), __dmul_rn(a.z, b.z)); }
+RT_DEV D3 dcross(D3 a, D3 b) {
+  return {__dsub_rn(__dmul_rn(a.y, b.z), __dmul_rn(a.z, b.y)), __dsub_rn(__dmul_rn(a.z, b.x), __dmul_rn(a.x, b.z)),
+          __dsub_rn(__dmul_rn(a.x, b.y), __dmul_rn(a.y, b.x))};
+}
+
+// The ray in object space in f64, from the instance's f32 rows (the f64 reference's TLAS
+// wrapper: left-to-right sums of f64 products).
+template <uint32_t LAYOUT>
+RT_DEV void ray64(const uint32_t* __restrict__ w, uint32_t inst, const Ray& ray, D3& o, D3& d) {
+  const size_t r = LAYOUT == 0 ? 16 + (size_t)inst * 32 : 8 + (size_t)inst * 24;
+  double m[12];
+#pragma unroll
+  for (int k = 0; k < 12; ++k) m[k] = (double)ldf(w, r + k);
+  const D3 wo = {ray.o.x, ray.o.y, ray.o.z}, wd = {ray.d.x, ray.d.y, ray.d.z};
+  o = {__dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[0], wo.x), __dmul_rn(m[1], wo.y)), __dmul_rn(m[2], wo.z)), m[3]),
+       __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[4], wo.x), __dmul_rn(m[5], wo.y)), __dmul_rn(m[6], wo.z)), m[7]),
+       __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(m[8], wo.x), __dmul_rn(m[9], wo.y)), __dmul_rn(m[10], wo.z)), m[11])};
+  d = {__dadd_rn(__dadd_rn(__dmul_rn(m[0], wd.x), __dmul_rn(m[1], wd.y)), __dmul_rn(m[2], wd.z)),
+       __dadd_rn(__dadd_rn(__dmul_rn(m[4], wd.x), __dmul_rn(m[5], wd.y)), __dmul_rn(m[6], wd.z)),
+       __dadd_rn(__dadd_rn(__dmul_rn(m[8], wd.x), __dmul_rn(m[9], wd.y)), __dmul_rn(m[10], wd.z))};
+}
+
+// f64 Möller-Trumbore over the source triangle at word `ref` (reference.rs:121-158). The
+// reflection layout's triangle is a, a + e1, a + e2 with e1/e2 as stored; the GI layout's is
+// three indexed positions. Accepts t in (tmin, tmax).
+template <uint32_t LAYOUT>
+__device__ __noinline__ bool mt64(const uint32_t* __restrict__ w, uint32_t inst, uint32_t ref, const Ray& ray, double& t, double& u,
+                 double& v) {
+  D3 o, d;
+  ray64<LAYOUT>(w, inst, ray, o, d);
+  D3 a, ab, ac;
+  if (LAYOUT == 1) {
+    a = {ldf(w, ref), ldf(w, ref + 1), ldf(w, ref + 2)};
+    ab = {ldf(w, ref + 3), ldf(w, ref + 4), ldf(w, ref + 5)};
+    ac = {ldf(w, ref + 6), ldf(w, ref + 7), ldf(w, ref + 8)};
+  } else {
+    const size_t positions = ld(w, 16 + (size_t)inst * 32 + 20);
+    const uint32_t ia = ld(w, ref), ib = ld(w, ref + 1), ic = ld(w, ref + 2);
+    a = {ldf(w, positions + 3 * (size_t)ia), ldf(w, positions + 3 * (size_t)ia + 1), ldf(w, positions + 3 * (size_t)ia + 2)};
+    const D3 b = {ldf(w, positions + 3 * (size_t)ib), ldf(w, positions + 3 * (size_t)ib + 1), ldf(w, positions + 3 * (size_t)ib + 2)};
+    const D3 c = {ldf(w, positions + 3 * (size_t)ic), ldf(w, positions + 3 * (size_t)ic + 1), ldf(w, positions + 3 * (size_t)ic + 2)};
+    ab = dsub3(b, a);
+    ac = dsub3(c, a);
+  }
+  const D3 p = dcross(d, ac);
+  const double det = ddot(ab, p);
+  if (det == 0.0) return false;
+  const D3 s = dsub3(o, a);
+  u = __ddiv_rn(ddot(s, p), det);
+  if (!(u >= 0.0 && u <= 1.0)) return false;
+  const D3 q = dcross(s, ab);
+  v = __ddiv_rn(ddot(d, q), det);
+  if (v < 0.0 || __dadd_rn(u, v) > 1.0) return false;
+  t = __ddiv_rn(ddot(ac, q), det);
+  return t > (double)ray.tmin && t < (double)ray.tmax;
+}
+
+// Per-instance object-space ray state for the 8-wide walk.
+struct W8Ray {
+  F3 o, d, inv;
+  uint32_t oct;
+  // watertight shear rows: (Ax, Ay, Az) = M (v - o)
+  F3 mx, my, mz;
+  float omax;   // |o|_inf
+  float tscale; // 8 u |1 / d_kz|: absolute error of t per unit of coordinate magnitude
+  bool valid;
+};
+
+RT_DEV void w8_setup(W8Ray& R) {
+  R.inv = safe_inverse(R.d);
+  R.oct = (R.d.x < 0.0f ? 1u : 0u) | (R.d.y < 0.0f ? 2u : 0u) | (R.d.z < 0.0f ? 4u : 0u);
+  const float ax = fabsf(R.d.x), ay = fabsf(R.d.y), az = fabsf(R.d.z);
+  const int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
+  int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
+  auto comp = [&](int k) { return k == 0 ? R.d.x : (k == 1 ? R.d.y : R.d.z); };
+  const float dz = comp(kz);
+  if (dz < 0.0f) {
+    const int t = kx;
+    kx = ky;
+    ky = t;
+  }
+  R.valid = dz != 0.0f;
+  const float sz = R.valid ? __frcp_rn(dz) : 0.0f;
+  const float sx = __fmul_rn(comp(kx), sz), sy = __fmul_rn(comp(ky), sz);
+  // rows of the shear: M_x = e_kx - sx e_kz, M_y = e_ky - sy e_kz, M_z = sz e_kz
+  auto row = [&](int one, float at_z) {
+    return F3{one == 0 ? 1.0f : (kz == 0 ? at_z : 0.0f), one == 1 ? 1.0f : (kz == 1 ? at_z : 0.0f),
+              one == 2 ? 1.0f : (kz == 2 ? at_z : 0.0f)};
+  };
+  R.mx = row(kx, -sx);
+  R.my = row(ky, -sy);
+  R.mz = {kz == 0 ? sz : 0.0f, kz == 1 ? sz : 0.0f, kz == 2 ? sz : 0.0f};
+  R.omax = fmaxf(fmaxf(fabsf(R.o.x), fabsf(R.o.y)), fabsf(R.o.z));
+  R.tscale = 8.0f * W8_U * fabsf(sz);
+}
+
+// Projected vertex (Ax, Ay, Az): one fixed chain of operations per vertex.
+RT_DEV F3 w8_project(const W8Ray& R, F3 v) {
+  const F3 a = {__fsub_rn(v.x, R.o.x), __fsub_rn(v.y, R.o.y), __fsub_rn(v.z, R.o.z)};
+  return {__fmaf_rn(a.z, R.mx.z, __fmaf_rn(a.y, R.mx.y, __fmul_rn(a.x, R.mx.x))),
+          __fmaf_rn(a.z, R.my.z, __fmaf_rn(a.y, R.my.y, __fmul_rn(a.x, R.my.x))),
+          __fmaf_rn(a.z, R.mz.z, __fmaf_rn(a.y, R.mz.y, __fmul_rn(a.x, R.mz.x)))};
+}
+
+// An edge function, antisymmetric in its two vertices; exact zero recomputed in double.
+RT_DEV float w8_edge(float px, float py, float qx, float qy) {
+  float e = __fsub_rn(__fmul_rn(px, qy), __fmul_rn(py, qx));
+  if (e == 0.0f) e = (float)__dsub_rn((double)px * (double)qy, (double)py * (double)qx);
+  return e;
+}
+
+// Watertight test. Returns 0 miss, 1 hit, 2 uncertain (near an edge: the caller re-tests in
+// f64). On hit / uncertain, t, u, v hold the f32 estimate (t may be outside the range).
+RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v) {
+  const F3 A = w8_project(R, v0), B = w8_project(R, v1), C = w8_project(R, v2);
+  const float U = w8_edge(C.x, C.y, B.x, B.y);  // opposite v0
+  const float V = w8_edge(A.x, A.y, C.x, C.y);  // opposite v1
+  const float W = w8_edge(B.x, B.y, A.x, A.y);  // opposite v2
+  const float sum = __fadd_rn(__fadd_rn(fabsf(U), fabsf(V)), fabsf(W));
+  const float lim = __fmul_rn(W8_EDGE, sum);
+  const bool neg = U < 0.0f || V < 0.0f || W < 0.0f, pos = U > 0.0f || V > 0.0f || W > 0.0f;
+  int kind = 1;
+  if (neg && pos) {
+    // outside, unless every edge function of the wrong sign is tiny
+    const float s = (U + V + W) >= 0.0f ? 1.0f : -1.0f;
+    const bool near_edge = (s * U >= -lim) && (s * V >= -lim) && (s * W >= -lim);
+    if (!near_edge) return 0;
+    kind = 2;
+  }
+  const float det = __fadd_rn(__fadd_rn(U, V), W);
+  if (det == 0.0f) return sum > 0.0f ? 2 : 0;
+  if (fabsf(U) <= lim || fabsf(V) <= lim || fabsf(W) <= lim) kind = 2;
+  const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, A.z), __fmul_rn(V, B.z)), __fmul_rn(W, C.z));
+  const float rd = __frcp_rn(det);
+  t = __fmul_rn(T, rd);
+  u = __fmul_rn(V, rd);
+  v = __fmul_rn(W, rd);
+  return kind;
+}
+
+// Considers one candidate triangle; returns true when an any-hit query is satisfied.
+template <uint32_t LAYOUT, bool ANY>
+RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const W8Ray& R, const Ray& ray, uint32_t inst,
+                         uint32_t tri, W8Best& best) {
+  const uint4 q0 = __ldg(V.tris + 3 * (size_t)tri), q1 = __ldg(V.tris + 3 * (size_t)tri + 1),
+              q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
+  const F3 v0 = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
+  const F3 v1 = {__uint_as_float(q0.w), __uint_as_float(q1.x), __uint_as_float(q1.y)};
+  const F3 v2 = {__uint_as_float(q1.z), __uint_as_float(q1.w), __uint_as_float(q2.x)};
+  float t, u, v;
+  const int kind = w8_triangle(R, v0, v1, v2, t, u, v);
+  if (kind == 0) return false;
+  const uint32_t ident = q2.y, ref = q2.z;
+  const float tmin = ray.tmin, tmax = ray.tmax;
+  // How far the f32 t may be from the f64 one: relative W8_TIE, or the absolute rounding of
+  // v - o at this magnitude (dominant for short hits far from the origin).
+  const float vmax = fmaxf(fmaxf(fmaxf(fabsf(v0.x), fabsf(v0.y)), fmaxf(fabsf(v0.z), fabsf(v1.x))),
+                           fmaxf(fmaxf(fabsf(v1.y), fabsf(v1.z)), fmaxf(fmaxf(fabsf(v2.x), fabsf(v2.y)), fabsf(v2.z))));
+  const float abs_err = R.tscale * (R.omax + vmax);
+  const float band = fmaxf(W8_TIE * fabsf(t), abs_err);
+  // Clearly outside the range or clearly behind the current best: nothing to decide.
+  if (kind == 1) {
+    if (!(t > tmin - band) || !(t < tmax + band)) return false;
+    if (best.hit && t > best.t + band + best.band) return false;
+  }
+  const bool uncertain = kind == 2 || !(t > tmin + band) || !(t < tmax - band) ||
+                         (best.hit && t >= best.t - band - best.band);
+  double t64 = 0.0, u64 = 0.0, v64 = 0.0;
+  if (uncertain) {
+    if (!mt64<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) return false;
+    if (best.hit && !best.has64) {
+      // the incumbent needs its f64 result too
+      const uint4 b2 = __ldg(V.tris + 3 * (size_t)best.tri + 2);
+      double bt, bu, bv;
+      if (mt64<LAYOUT>(w, best.inst, b2.z, ray, bt, bu, bv)) {
+        best.t64 = bt, best.u = (float)bu, best.v = (float)bv, best.t = (float)bt, best.has64 = true, best.band = 0.0f;
+      } else {
+        best.hit = false;  // the f32 estimate was a false hit: drop it
+      }
+    }
+    if (best.hit) {
+      const bool better = t64 < best.t64 || (t64 == best.t64 && (inst < best.inst || (inst == best.inst && ident < best.ident)));
+      if (!better) return false;
+    }
+    best.hit = true, best.has64 = true, best.t64 = t64, best.t = (float)t64, best.u = (float)u64, best.v = (float)v64;
+    best.band = 0.0f;
+  } else {
+    best.hit = true, best.has64 = false, best.t = t, best.u = u, best.v = v, best.band = band;
+    best.abs_err = abs_err;
+  }
+  best.inst = inst, best.tri = tri, best.ident = ident;
+  return ANY;
+}
+
+// XOR-permute an 8-bit slot mask: bit k of the result is bit (k ^ o) of m.
+RT_DEV uint32_t oct_permute(uint32_t m, uint32_t o) {
+  if (o & 1u) m = ((m & 0x55u) << 1) | ((m & 0xAAu) >> 1);
+  if (o & 2u) m = ((m & 0x33u) << 2) | ((m & 0xCCu) >> 2);
+  if (o & 4u) m = ((m & 0x0Fu) << 4) | ((m & 0xF0u) >> 4);
+  return m;
+}
+
+RT_DEV float q_f(uint32_t word, uint32_t byte) {
+  return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, byte | 0x7540u)), 8388608.0f);
+}
+
+// The per-lane traversal state of the persistent WIDE8 kernel.
+struct W8Lane {
+  Ray ray;
+  F3 world_inv;
+  W8Best best;
+  uint32_t ray_id, phase;
+  uint32_t tsp, flat;
+  uint32_t inst;
+  W8Ray R;
+  uint32_t node;                     // next node to process, EMPTY: take one from the group
+  uint32_t g_base, g_bits, g_imask;  // current node group
+  uint32_t sp;
+};
+
+// One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
+// Returns true when an any-hit query is satisfied.
+template <uint32_t LAYOUT, bool ANY>
+RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st) {
+  const W8Ray& R = L.R;
+  const uint4* np = V.nodes + 5 * (size_t)L.node;
+  const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
+  const float px = __uint_as_float(a0.x), py = __uint_as_float(a0.y), pz = __uint_as_float(a0.z);
+  const float Ax = __fmul_rn(__uint_as_float((a0.w & 0xffu) << 23), R.inv.x);
+  const float Ay = __fmul_rn(__uint_as_float(((a0.w >> 8) & 0xffu) << 23), R.inv.y);
+  const float Az = __fmul_rn(__uint_as_float(((a0.w >> 16) & 0xffu) << 23), R.inv.z);
+  const float Bx = __fmul_rn(__fsub_rn(px, R.o.x), R.inv.x), By = __fmul_rn(__fsub_rn(py, R.o.y), R.inv.y),
+              Bz = __fmul_rn(__fsub_rn(pz, R.o.z), R.inv.z);
+  // Per axis, |error of a plane's t| <= u (255 |A| + 3 |B|) + u |t| (the rounding of 1/d, of
+  // p - o, of (p - o) / d and of the fma). The absolute part, doubled and with |B| taken four
+  // times to cover rounding B -/+ E itself, moves the near planes down and the far planes up;
+  // the relative part is applied to the entry / exit after the max / min.
+  const float Ex = 2.0f * W8_U * fmaf(255.0f, fabsf(Ax), 4.0f * fabsf(Bx));
+  const float Ey = 2.0f * W8_U * fmaf(255.0f, fabsf(Ay), 4.0f * fabsf(By));
+  const float Ez = 2.0f * W8_U * fmaf(255.0f, fabsf(Az), 4.0f * fabsf(Bz));
+  const float Bnx = Bx - Ex, Bfx = Bx + Ex, Bny = By - Ey, Bfy = By + Ey, Bnz = Bz - Ez, Bfz = Bz + Ez;
+  const uint32_t imask = a0.w >> 24;
+  const uint32_t child_base = a1.x, tri_base = a1.y, meta_lo = a1.z, meta_hi = a1.w;
+  // near / far planes per axis by the direction's sign
+  const uint32_t nx0 = R.oct & 1u ? a3.z : a2.x, nx1 = R.oct & 1u ? a3.w : a2.y;
+  const uint32_t fx0 = R.oct & 1u ? a2.x : a3.z, fx1 = R.oct & 1u ? a2.y : a3.w;
+  const uint32_t ny0 = R.oct & 2u ? a4.x : a2.z, ny1 = R.oct & 2u ? a4.y : a2.w;
+  const uint32_t fy0 = R.oct & 2u ? a2.z : a4.x, fy1 = R.oct & 2u ? a2.w : a4.y;
+  const uint32_t nz0 = R.oct & 4u ? a4.z : a3.x, nz1 = R.oct & 4u ? a4.w : a3.y;
+  const uint32_t fz0 = R.oct & 4u ? a3.x : a4.z, fz1 = R.oct & 4u ? a3.y : a4.w;
+  const W8Best& best = L.best;
+  const float lim = best.hit ? best.t + 2.0f * best.band + W8_TIE * best.t : L.ray.tmax;
+  const float tmin = L.ray.tmin;
+  uint32_t hits = 0;
+#pragma unroll
+  for (int s = 0; s < 8; ++s) {
+    const uint32_t b = s & 3;
+    const float tnx = fmaf(q_f(s < 4 ? nx0 : nx1, b), Ax, Bnx), tfx = fmaf(q_f(s < 4 ? fx0 : fx1, b), Ax, Bfx);
+    const float tny = fmaf(q_f(s < 4 ? ny0 : ny1, b), Ay, Bny), tfy = fmaf(q_f(s < 4 ? fy0 : fy1, b), Ay, Bfy);
+    const float tnz = fmaf(q_f(s < 4 ? nz0 : nz1, b), Az, Bnz), tfz = fmaf(q_f(s < 4 ? fz0 : fz1, b), Az, Bfz);
+    float tn = fmaxf(fmaxf(tnx, tny), tnz), tf = fminf(fminf(tfx, tfy), tfz);
+    tn = fmaf(-2.0f * W8_U, fabsf(tn), tn);
+    tf = fmaf(2.0f * W8_U, fabsf(tf), tf);
+    if (fmaxf(tn, tmin) <= fminf(tf, lim)) hits |= 1u << s;
+  }
+  // A slot is a leaf when its meta byte has a count; empty slots have neither.
+  const uint32_t leafmask = ((meta_lo & 0xe0u) ? 1u : 0u) | ((meta_lo & 0xe000u) ? 2u : 0u) |
+                            ((meta_lo & 0xe00000u) ? 4u : 0u) | ((meta_lo & 0xe0000000u) ? 8u : 0u) |
+                            ((meta_hi & 0xe0u) ? 16u : 0u) | ((meta_hi & 0xe000u) ? 32u : 0u) |
+                            ((meta_hi & 0xe00000u) ? 64u : 0u) | ((meta_hi & 0xe0000000u) ? 128u : 0u);
+  uint32_t leaf_hits = hits & leafmask;
+  while (leaf_hits) {
+    const uint32_t s = __ffs(leaf_hits) - 1;
+    leaf_hits &= leaf_hits - 1;
+    const uint32_t m = ((s < 4 ? meta_lo : meta_hi) >> (8 * (s & 3))) & 0xffu;
+    const uint32_t first = tri_base + (m & 31u), count = m >> 5;
+    for (uint32_t k = 0; k < count; ++k)
+      if (w8_candidate<LAYOUT, ANY>(w, V, R, L.ray, L.inst, first + k, L.best)) return true;
+  }
+  const uint32_t inner = oct_permute(hits & imask, R.oct);
+  if (inner) {
+    if (L.g_bits) {
+      if (L.sp < W8_STACK) stack[L.sp++] = make_uint2(L.g_base, L.g_bits | L.g_imask << 8);
+      else atomicAdd(&st->stack_drops, 1ull);
+    }
+    L.g_base = child_base, L.g_bits = inner, L.g_imask = imask;
+  }
+  L.node = EMPTY;
+  return false;
+}
+
+// The next node of the current group (or of a popped one); false when the BLAS is done.
+RT_DEV bool w8_next(W8Lane& L, const uint2* stack) {
+  while (L.g_bits == 0) {
+    if (L.sp == 0) return false;
+    const uint2 e = stack[--L.sp];
+    L.g_base = e.x, L.g_bits = e.y & 0xffu, L.g_imask = e.y >> 8;
+  }
+  const uint32_t k = __ffs(L.g_bits) - 1;
+  L.g_bits &= L.g_bits - 1;
+  const uint32_t slot = k ^ L.R.oct;
+  L.node = L.g_base + __popc(L.g_imask & ((1u << slot) - 1u));
+  return true;
+}
+
+// Enters instance i when its world box survives; sets up the object-space ray.
+template <uint32_t LAYOUT, bool ANY>
+RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i) {
+  const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;
+  if (ANY && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
+  const W8Best& best = L.best;
+  const float bound = best.hit ? best.t + 2.0f * best.band + 2.0f * W8_TIE * best.t : L.ray.tmax;
+  if (!(slab_near(L.ray.o, L.world_inv, ld3(w, r + 12), ld3(w, r + 15), L.ray.tmin, bound) <= bound)) return;
+  const uint32_t root = __ldg(V.inst + 2 * (size_t)i);
+  if (root == EMPTY) return;
+  const float r00 = ldf(w, r), r01 = ldf(w, r + 1), r02 = ldf(w, r + 2), r03 = ldf(w, r + 3);
+  const float r10 = ldf(w, r + 4), r11 = ldf(w, r + 5), r12 = ldf(w, r + 6), r13 = ldf(w, r + 7);
+  const float r20 = ldf(w, r + 8), r21 = ldf(w, r + 9), r22 = ldf(w, r + 10), r23 = ldf(w, r + 11);
+  L.R.o = {dot4p(r00, r01, r02, r03, L.ray.o), dot4p(r10, r11, r12, r13, L.ray.o), dot4p(r20, r21, r22, r23, L.ray.o)};
+  L.R.d = {dot3({r00, r01, r02}, L.ray.d), dot3({r10, r11, r12}, L.ray.d), dot3({r20, r21, r22}, L.ray.d)};
+  w8_setup(L.R);
+  if (!L.R.valid) return;
+  L.inst = i;
+  L.node = root;
+  L.g_bits = 0;
+  L.sp = 0;
+  L.phase = 2;
+}
+
+template <uint32_t LAYOUT, bool ANY>
+RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, void* __restrict__ out) {
+  W8Best& b = L.best;
+  const uint32_t id = L.ray_id;
+  L.phase = 0;
+  if (ANY) {
+    reinterpret_cast<uint32_t*>(out)[id] = b.hit ? 1u : 0u;
+    return;
+  }
+  if (b.hit && !b.has64 && b.abs_err > 2e-6f * b.t) {
+    // the f32 t is not within 1e-5 relative: report the f64 one
+    const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(V.tris) + 12 * (size_t)b.tri + 10);
+    double t64, u64, v64;
+    if (mt64<LAYOUT>(w, b.inst, ref, L.ray, t64, u64, v64)) b.t = (float)t64, b.u = (float)u64, b.v = (float)v64;
+  }
+  if (LAYOUT == 1) {
+    uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * (size_t)id;
+    o[0] = __float_as_uint(b.t);
+    o[1] = b.hit ? ld(w, 8 + 24 * (size_t)b.inst + 21) + 1 : 0u;
+    o[2] = b.hit ? b.ident : 0u;
+    o[3] = b.hit ? __float_as_uint(b.u) : 0u;
+    o[4] = b.hit ? __float_as_uint(b.v) : 0u;
+    return;
+  }
+  uint32_t* o = reinterpret_cast<uint32_t*>(out) + 10 * (size_t)id;
+  if (!b.hit) {
+    o[0] = __float_as_uint(L.ray.tmax), o[1] = EMPTY, o[2] = o[3] = o[4] = 0;
+    o[5] = o[6] = 0, o[7] = o[8] = o[9] = 0;
+    return;
+  }
+  const size_t r = 16 + 32 * (size_t)b.inst;
+  const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(V.tris) + 12 * (size_t)b.tri + 10);
+  const uint32_t prim_base = ld(w, r + 28), positions = ld(w, r + 20);
+  const uint32_t ia = ld(w, ref), ib = ld(w, ref + 1), ic = ld(w, ref + 2);
+  const F3 a = ld3(w, positions + 3 * (size_t)ia), bb = ld3(w, positions + 3 * (size_t)ib), c = ld3(w, positions + 3 * (size_t)ic);
+  const F3 cr = cross3(sub3(bb, a), sub3(c, a));
+  const float m0 = ldf(w, r), m1 = ldf(w, r + 1), m2 = ldf(w, r + 2), m4 = ldf(w, r + 4), m5 = ldf(w, r + 5),
+              m6 = ldf(w, r + 6), m8 = ldf(w, r + 8), m9 = ldf(w, r + 9), m10 = ldf(w, r + 10);
+  const F3 nrm = unit_normal({add(add(mul(m0, cr.x), mul(m4, cr.y)), mul(m8, cr.z)),
+                              add(add(mul(m1, cr.x), mul(m5, cr.y)), mul(m9, cr.z)),
+                              add(add(mul(m2, cr.x), mul(m6, cr.y)), mul(m10, cr.z))});
+  o[0] = __float_as_uint(b.t), o[1] = b.inst;
+  if (prim_base != 0) o[2] = ld(w, prim_base + b.ident), o[3] = 0, o[4] = 0;
+  else o[2] = ia, o[3] = ib, o[4] = ic;
+  o[5] = __float_as_uint(b.u), o[6] = __float_as_uint(b.v);
+  o[7] = __float_as_uint(nrm.x), o[8] = __float_as_uint(nrm.y), o[9] = __float_as_uint(nrm.z);
+}
+
+// Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
+// step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
+// re-converges at the top of the loop.
+template <uint32_t LAYOUT, bool ANY, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__ w, W8View V, const float4* __restrict__ rays,
+                                                 const uint32_t* __restrict__ order, void* __restrict__ out,
+                                                 unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
+  uint2 stack[W8_STACK];
+  uint32_t tstack[STACK];
+  W8Lane L;
+  L.phase = 0;
+  const uint32_t count = ld(w, 0), top = ld(w, 1), root = ld(w, 2);
+  const size_t top_base = LAYOUT == 0 ? top : (top & ~3u);
+  bool drained = false;
+  for (;;) {
+    __syncwarp();
+    // ray refill (warp-aggregated)
+    const unsigned want = __ballot_sync(0xffffffffu, L.phase == 0 && !drained);
+    uint32_t id = EMPTY;
+    if (want) {
+      const int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
+      uint32_t base = 0;
+      if (lane == leader) base = atomicAdd(counter, (unsigned)__popc(want));
+      base = __shfl_sync(0xffffffffu, base, leader);
+      if (base + (uint32_t)__popc(want) >= n) drained = true;
+      const uint32_t idx = base + __popc(want & ((1u << lane) - 1u));
+      if ((want >> lane & 1u) && idx < n) id = idx;
+    }
+    if (id != EMPTY) {
+      L.ray_id = order ? __ldg(order + id) : id;
+      L.ray = load_ray(rays, L.ray_id);
+      L.world_inv = safe_inverse(L.ray.d);
+      W8Best& b = L.best;
+      b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.abs_err = 0.0f, b.t64 = 0.0;
+      b.inst = EMPTY, b.tri = 0, b.ident = 0, b.u = b.v = 0.0f;
+      L.phase = 1;
+      L.flat = 0;
+      L.tsp = 0;
+      if (top != 0 && count != 0) tstack[L.tsp++] = root;
+    }
+    if (!__any_sync(0xffffffffu, L.phase != 0)) {
+      if (drained) break;
+      continue;
+    }
+    if (L.phase == 2) {
+      if (L.node == EMPTY && !w8_next(L, stack)) {
+        L.phase = 1;
+      } else {
+        if (w8_node<LAYOUT, ANY>(w, V, L, stack, st)) w8_finish<LAYOUT, ANY>(w, V, L, out);
+        continue;
+      }
+    }
+    if (L.phase == 1) {
+      if (top == 0) {
+        if (L.flat >= count) {
+          w8_finish<LAYOUT, ANY>(w, V, L, out);
+          continue;
+        }
+        w8_enter<LAYOUT, ANY>(w, V, L, L.flat++);
+        continue;
+      }
+      if (L.tsp == 0) {
+        w8_finish<LAYOUT, ANY>(w, V, L, out);
+        continue;
+      }
+      const uint32_t item = tstack[--L.tsp];
+      if (item & LEAF) {
+        w8_enter<LAYOUT, ANY>(w, V, L, item & ~LEAF);
+        continue;
+      }
+      const W8Best& b = L.best;
+      const float bound = b.hit ? b.t + 2.0f * b.band + 2.0f * W8_TIE * b.t : b.t;
+      top_step(w, top_base + (size_t)item * 32, L.ray, L.world_inv, bound, tstack, L.tsp, st);
+    }
+  }
+}
+
+}  // namespace rtk

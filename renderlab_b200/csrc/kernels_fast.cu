@@ -1,13 +1,62 @@
-// FAST kernels: the PLAIN arithmetic (bit-exact) under a scheduled launch.
-#include "kernels/plain.cuh"
+// Launchers for the FAST kernels: persistent grids sized to fill every SM once.
+#include <cuda_runtime.h>
+
+#include "kernels/fast.cuh"
 #include "launch.hpp"
 
 namespace rtl {
 
+namespace {
+constexpr int FAST_BLOCK = 128;
+
+// Resident blocks of `kernel` on the whole device, queried once per kernel (one device type).
+template <class K>
+cudaError_t resident_blocks(K kernel, uint32_t& out) {
+  static uint32_t cached = 0;
+  if (cached) {
+    out = cached;
+    return cudaSuccess;
+  }
+  int dev = 0, sms = 0, per_sm = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, FAST_BLOCK, 0)) != cudaSuccess) return e;
+  cached = out = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+  return cudaSuccess;
+}
+
+template <class K>
+cudaError_t grid_for(K kernel, uint32_t n, dim3& grid) {
+  uint32_t full = 0;
+  cudaError_t e = resident_blocks(kernel, full);
+  if (e != cudaSuccess) return e;
+  const uint32_t need = (n + FAST_BLOCK - 1) / FAST_BLOCK;
+  grid = dim3(need < full ? need : full);
+  return cudaSuccess;
+}
+
+template <class K>
+cudaError_t run(K kernel, const SceneView& s, const float4* rays, const uint32_t* order, void* hits, uint32_t n,
+                unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+  dim3 grid;
+  cudaError_t e = grid_for(kernel, n, grid);
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+  kernel<<<grid, FAST_BLOCK, 0, stream>>>(s.words, rays, order, hits, rtk::RayQueue{counter, n}, st);
+  return cudaGetLastError();
+}
+}  // namespace
+
 cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                        uint32_t n, rtk::DevStatus* st, cudaStream_t stream) {
-  (void)s, (void)mode, (void)rays, (void)order, (void)hits, (void)n, (void)st, (void)stream;
-  return cudaErrorNotSupported;
+                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  if (s.layout == 0) {
+    if (mode == 0) return run(rtk::k_gi_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
+    return run(rtk::k_gi_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
+  }
+  if (mode == 0) return run(rtk::k_rs_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
+  return run(rtk::k_rs_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
 }
 
 }  // namespace rtl

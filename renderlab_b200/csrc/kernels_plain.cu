@@ -9,7 +9,7 @@ constexpr uint32_t PLAIN_BLOCK = 128;
 
 __global__ void k_selftest(uint32_t* out) {
   if (threadIdx.x != 0 || blockIdx.x != 0) return;
-  volatile float pz = 0.0f, nz = -0.0f, three = 3.0f, two = 2.0f, tiny = 1e-40f;
+  volatile float pz = 0.0f, nz = -0.0f, three = 3.0f, two = 2.0f, tiny = 5.877471754e-39f;  // 2^-127, subnormal
   out[0] = __float_as_uint(fminf(nz, pz));
   out[1] = __float_as_uint(fminf(pz, nz));
   out[2] = __float_as_uint(fmaxf(nz, pz));

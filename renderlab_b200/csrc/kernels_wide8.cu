@@ -1,0 +1,55 @@
+// Launchers for the WIDE8 kernels.
+#include "kernels/wide8.cuh"
+#include "launch.hpp"
+
+namespace rtl {
+
+namespace {
+constexpr int W8_BLOCK = 128;
+}
+
+template <class K>
+cudaError_t resident(K kernel, uint32_t& out) {
+  static uint32_t cached = 0;
+  if (!cached) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, W8_BLOCK, 0);
+    if (e != cudaSuccess) return e;
+    cached = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+  }
+  out = cached;
+  return cudaSuccess;
+}
+
+template <class K>
+cudaError_t run(K kernel, const uint32_t* words, const rtk::W8View& v, const float4* rays, const uint32_t* order,
+                void* hits, unsigned int* counter, uint32_t n, rtk::DevStatus* st, cudaStream_t stream) {
+  uint32_t full = 0;
+  cudaError_t e = resident(kernel, full);
+  if (e != cudaSuccess) return e;
+  const uint32_t need = (n + W8_BLOCK - 1) / W8_BLOCK;
+  if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+  kernel<<<need < full ? need : full, W8_BLOCK, 0, stream>>>(words, v, rays, order, hits, counter, n, st);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
+                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  if (!s.wide8) return cudaErrorInvalidValue;
+  rtk::W8View v;
+  const uint32_t* base = static_cast<const uint32_t*>(s.wide8);
+  v.nodes = reinterpret_cast<const uint4*>(base + s.w8_nodes_at);
+  v.tris = reinterpret_cast<const uint4*>(base + s.w8_tris_at);
+  v.inst = base + s.w8_inst_at;
+  if (s.layout == 0) {
+    if (mode == 0) return run(rtk::k_wide8<0, false, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
+    return run(rtk::k_wide8<0, true, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
+  }
+  if (mode == 0) return run(rtk::k_wide8<1, false, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
+  return run(rtk::k_wide8<1, true, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
+}
+
+}  // namespace rtl

@@ -14,17 +14,23 @@ struct SceneView {
   size_t n_words;
   uint32_t instances;
   uint32_t top;
-  // Derived 8-wide layout for the WIDE8 kernel (null until built).
+  // Derived 8-wide layout for the WIDE8 kernel (null until rt_scene_prepare): one device
+  // allocation holding nodes, triangles and the per-instance table at these word offsets.
   const void* wide8;
   size_t wide8_bytes;
+  size_t w8_nodes_at, w8_tris_at, w8_inst_at;
 };
 
 // PLAIN: mode 0 closest, 1/2 any-hit. Hits as documented in rt_trace.h.
 cudaError_t launch_plain(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                          rtk::DevStatus* st, cudaStream_t stream);
 // FAST: bit-exact with PLAIN; `order` (optional) permutes which ray each thread traces.
+// `counter` is a device word the launch owns until it completes (zeroed on `stream`).
 cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                        uint32_t n, rtk::DevStatus* st, cudaStream_t stream);
+                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream);
+// WIDE8: the precision variant over the scene's derived 8-wide layout.
+cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
+                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream);
 cudaError_t launch_selftest(uint32_t* out16, cudaStream_t stream);
 
 }  // namespace rtl

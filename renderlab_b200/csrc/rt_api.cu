@@ -13,6 +13,7 @@
 
 #include "../../include/rt_trace.h"
 #include "host/host.hpp"
+#include "host/wide8.hpp"
 #include "launch.hpp"
 
 struct rt_scene {
@@ -23,6 +24,7 @@ struct rt_scene {
   size_t device_bytes = 0;
   void* d_wide8 = nullptr;
   size_t wide8_bytes = 0;
+  size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
 };
 
 struct rt_blas {
@@ -33,6 +35,10 @@ struct rt_ctx {
   int device = 0;
   rtk::DevStatus* d_status = nullptr;
   uint32_t* d_scratch = nullptr;  // 16 words for the self-test
+  // Ray counters of persistent launches: launch k uses slot k mod COUNTER_SLOTS, so up to that
+  // many launches may be in flight at once across streams.
+  unsigned int* d_counters = nullptr;
+  std::atomic<uint64_t> counter_seq{0};
   std::mutex mu;
   std::string last_error;
   std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
@@ -47,6 +53,7 @@ namespace {
 
 constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BYTES = 32;
 constexpr uint32_t HOST_CHUNK = 1u << 20;
+constexpr uint32_t COUNTER_SLOTS = 4096;
 
 rt_status fail(rt_ctx* ctx, rt_status s, const char* fmt, ...) {
   if (ctx) {
@@ -80,6 +87,7 @@ rtl::SceneView view_of(const rt_scene* s) {
   v.top = s->info.top;
   v.wide8 = s->d_wide8;
   v.wide8_bytes = s->wide8_bytes;
+  v.w8_nodes_at = s->w8_nodes_at, v.w8_tris_at = s->w8_tris_at, v.w8_inst_at = s->w8_inst_at;
   return v;
 }
 
@@ -94,7 +102,14 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
       e = rtl::launch_plain(v, (uint32_t)mode, r, hits, n, ctx->d_status, stream);
       break;
     case RT_KERNEL_FAST:
-      e = rtl::launch_fast(v, (uint32_t)mode, r, order, hits, n, ctx->d_status, stream);
+      e = rtl::launch_fast(v, (uint32_t)mode, r, order, hits, n,
+                           ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream);
+      break;
+    case RT_KERNEL_WIDE8:
+      if (!scene->d_wide8)
+        return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
+      e = rtl::launch_wide8(v, (uint32_t)mode, r, order, hits, n,
+                            ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream);
       break;
     default:
       return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
@@ -129,6 +144,7 @@ rt_status rt_ctx_create(int device, rt_ctx** out) {
   if (cudaMalloc(&ctx->d_status, sizeof(rtk::DevStatus)) != cudaSuccess) return RT_ERR_OOM;
   if (cudaMemset(ctx->d_status, 0, sizeof(rtk::DevStatus)) != cudaSuccess) return RT_ERR_CUDA;
   if (cudaMalloc(&ctx->d_scratch, 64) != cudaSuccess) return RT_ERR_OOM;
+  if (cudaMalloc(&ctx->d_counters, COUNTER_SLOTS * sizeof(unsigned int)) != cudaSuccess) return RT_ERR_OOM;
   for (auto& s : ctx->streams)
     if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return RT_ERR_CUDA;
   *out = ctx.release();
@@ -142,6 +158,7 @@ void rt_ctx_destroy(rt_ctx* ctx) {
     if (s) cudaStreamSynchronize(s), cudaStreamDestroy(s);
   cudaFree(ctx->d_status);
   cudaFree(ctx->d_scratch);
+  cudaFree(ctx->d_counters);
   cudaFree(ctx->d_rays);
   cudaFree(ctx->d_hits);
   delete ctx;
@@ -226,6 +243,44 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
     return fail(ctx, RT_ERR_LAYOUT, "records rejected: %s", err.c_str());
   RT_CUDA(ctx, cudaMemcpy(scene->d_words, words, n_words * 4, cudaMemcpyHostToDevice));
   scene->info = info;
+  return RT_OK;
+}
+
+rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
+  if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if (kernel != RT_KERNEL_WIDE8) return RT_OK;  // PLAIN and FAST read the packed words directly
+  if (scene->d_wide8) return RT_OK;
+  std::vector<uint32_t> words(scene->n_words);
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, cudaMemcpy(words.data(), scene->d_words, scene->n_words * 4, cudaMemcpyDeviceToHost));
+  rtb::Wide8Scene w8;
+  std::string err;
+  const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  if (!rtb::build_wide8_scene(scene->layout, words.data(), words.size(), w8, err, threads))
+    return fail(ctx, RT_ERR_LAYOUT, "8-wide build: %s", err.c_str());
+  // one allocation: nodes | triangles | instance table, each 16-byte aligned
+  auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
+  const size_t nodes_at = 0, tris_at = up4(w8.nodes.size()), inst_at = tris_at + up4(w8.tris.size());
+  const size_t total = inst_at + up4(std::max<size_t>(w8.inst.size(), 1));
+  void* d = nullptr;
+  if (cudaMalloc(&d, total * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RT_ERR_OOM, "device allocation of %zu bytes for the 8-wide layout failed", total * 4);
+  }
+  cudaError_t e = cudaMemcpy(static_cast<uint32_t*>(d) + nodes_at, w8.nodes.data(), w8.nodes.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(static_cast<uint32_t*>(d) + tris_at, w8.tris.data(), w8.tris.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !w8.inst.empty())
+    e = cudaMemcpy(static_cast<uint32_t*>(d) + inst_at, w8.inst.data(), w8.inst.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return fail(ctx, RT_ERR_CUDA, "8-wide upload: %s", cudaGetErrorString(e));
+  }
+  scene->d_wide8 = d;
+  scene->wide8_bytes = total * 4;
+  scene->w8_nodes_at = nodes_at, scene->w8_tris_at = tris_at, scene->w8_inst_at = inst_at;
+  scene->device_bytes += scene->wide8_bytes;
+  ctx->scene_bytes += scene->wide8_bytes;
   return RT_OK;
 }
 

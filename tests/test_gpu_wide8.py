@@ -1,0 +1,133 @@
+"""GPU parity of the WIDE8 kernel (compressed 8-wide BVH, watertight f32 tests, f64 re-test of
+uncertain candidates) against the FP64 oracle (crates/asset/src/cluster_bvh/reference.rs
+restated over the packed buffers).
+
+Tolerances: hit identity must equal the FP64 oracle's except on near ties, defined as both
+hitting with |t - t64| <= 1e-6 * t64; t within 1e-5 relative of t64 on every hit; any-hit
+flags equal except where the FP64 hit lies within 1e-5 relative of tmin or tmax."""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from renderlab_b200 import api as A
+from renderlab_b200 import scenes as S
+
+from . import helpers as H
+from .test_gpu_parity import gpu_trace, product_words
+
+pytestmark = pytest.mark.gpu
+
+T_REL = 1e-5
+TIE_REL = 1e-6
+
+
+def check_closest(layout, got, ref64, ident64, what):
+    """Returns (max rel t error, mean rel t error, near ties) and asserts the bar."""
+    if layout == A.LAYOUT_GI:
+        ghit = got[:, 1] != A.MISS
+        gid = got[:, 1:5]
+        oid = ident64[:, 2:6]
+    else:
+        ghit = got[:, 1] != 0
+        gid = got[:, 1:3]
+        oid = ident64[:, 2:4]
+    ohit = ref64[:, 0] > 0
+    t = got[:, 0].view(np.float32).astype(np.float64)
+    t64 = ref64[:, 1]
+    both = ghit & ohit
+    rel = np.abs(t[both] - t64[both]) / np.maximum(np.abs(t64[both]), 1e-30)
+    same_id = (gid == oid).all(axis=1)
+    mism = (ghit != ohit) | (both & ~same_id)
+    tie = mism & both & (np.abs(t - t64) <= TIE_REL * np.abs(t64))
+    bad = np.nonzero(mism & ~tie)[0]
+    assert len(bad) == 0, (f"{what}: {len(bad)} unexplained mismatches of {len(got)}; first {bad[:4]}: "
+                           f"got {got[bad[:2]]} oracle hit {ohit[bad[:2]]} t64 {t64[bad[:2]]} ident {oid[bad[:2]]}")
+    if both.any():
+        assert rel.max() <= T_REL, f"{what}: max rel t error {rel.max():.3g}"
+    return (float(rel.max()) if both.any() else 0.0, float(rel.mean()) if both.any() else 0.0, int(tie.sum()))
+
+
+def check_any(got, rays, ref64, what):
+    ohit = ref64[:, 0] > 0
+    ghit = got != 0
+    mism = ghit != ohit
+    t64 = ref64[:, 1]
+    near = ohit & ((np.abs(t64 - rays[:, 7]) <= T_REL * np.abs(rays[:, 7])) | (np.abs(t64 - rays[:, 3]) <= T_REL * np.maximum(np.abs(rays[:, 3]), 1e-30)))
+    bad = np.nonzero(mism & ~near)[0]
+    assert len(bad) == 0, f"{what}: {len(bad)} any-hit mismatches; first {bad[:4]}"
+
+
+def traced(engine, layout, words, rays, mode):
+    scene = engine.upload(layout, words)
+    try:
+        scene.prepare("wide8")
+        return gpu_trace(engine, scene, rays, mode, "wide8")
+    finally:
+        scene.release()
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_wide8_clusters_primary_and_gi(engine, layout):
+    mesh, rays = H.small_clusters(60_000, 256, 256)
+    prims = [True] if layout == A.LAYOUT_GI else None
+    w = product_words(layout, [mesh], S.identity_instances(1), primitives=prims)
+    got = traced(engine, layout, w, rays, A.CLOSEST)
+    ref, ident = O.fp64_trace(w, rays, layout)
+    stats = check_closest(layout, got, ref, ident, "primary")
+    hit = ref[:, 0] > 0
+    pts = S.hit_points(rays[hit], ref[hit, 1].astype(np.float32))
+    prim = ident[hit, 1]
+    gi = S.hemisphere_rays(pts, S.triangle_normals(mesh, prim if layout == A.LAYOUT_REFLECTION else ident[hit, 1]),
+                           rays[hit, 4:7], 40_000, S.Stream(77))
+    got = traced(engine, layout, w, gi, A.CLOSEST)
+    ref, ident = O.fp64_trace(w, gi, layout)
+    stats_gi = check_closest(layout, got, ref, ident, "gi")
+    print("wide8 t error (max, mean, ties)", stats, stats_gi)
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_wide8_instanced_cubes(engine, layout):
+    mesh, inst = S.cubes_instanced(30)
+    inst.casts = (np.arange(len(inst)) % 5) != 2
+    w = product_words(layout, [mesh], inst)
+    rays = H.small_cubes(30, 160, 160)[1]
+    got = traced(engine, layout, w, rays, A.CLOSEST)
+    ref, ident = O.fp64_trace(w, rays, layout)
+    check_closest(layout, got, ref, ident, "closest")
+    hit = ref[:, 0] > 0
+    sun = S.sun_rays(S.hit_points(rays[hit], ref[hit, 1].astype(np.float32)))
+    got = traced(engine, layout, w, sun, A.ANY_CASTERS)
+    ref_any, _ = O.fp64_trace(w, sun, layout, any_hit=True)
+    check_any(got, sun, ref_any, "sun")
+
+
+def test_wide8_edge_rays(engine):
+    p, i = H.grid(12)
+    mesh = S.Mesh(p, i)
+    rays = []
+    for d in ([0, -1, 0], [0, 1, 0], [1, 0, 0], [0.3, -1, 0], [0, -1, 1e-31], [1e-35, -1, 0]):
+        for o in ([0.5, 1, 0.5], [0.0, 0.5, 0.0], [0.25, 0.0, 0.25], [1.0, 2.0, 1.0], [1 / 3, 1, 0.5]):
+            for tmin, tmax in ((0.0, 1e30), (0.0, np.inf), (0.0, 3.4028235e38), (0.5, 0.25), (1e-4, 10.0)):
+                rays.append([*o, tmin, *d, tmax])
+    rays = np.array(rays, np.float32)
+    for layout in (A.LAYOUT_GI, A.LAYOUT_REFLECTION):
+        w = product_words(layout, [mesh], S.identity_instances(1))
+        got = traced(engine, layout, w, rays, A.CLOSEST)
+        ref, ident = O.fp64_trace(w, rays, layout)
+        check_closest(layout, got, ref, ident, f"edge rays layout {layout}")
+
+
+def test_wide8_grid_edges_are_watertight(engine):
+    """Rays aimed exactly at shared edges and vertices of a grid: none slips through."""
+    p, i = H.grid(16)
+    mesh = S.Mesh(p * np.float32(4.0), i)
+    xs = np.arange(17, dtype=np.float32) / 16 * 4
+    o = np.array([[x, 1.0, z] for x in xs[1:-1] for z in np.concatenate([xs[1:-1], xs[1:-1] + 0.125])], np.float32)
+    rays = S.pack_rays(o, np.tile([0.0, -1.0, 0.0], (len(o), 1)), 0.0, 10.0)
+    for layout in (A.LAYOUT_GI, A.LAYOUT_REFLECTION):
+        w = product_words(layout, [mesh], S.identity_instances(1))
+        got = traced(engine, layout, w, rays, A.CLOSEST)
+        hit = got[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)
+        assert hit.all(), f"{(~hit).sum()} rays slipped through the grid"
