@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--width", type=int, default=2048)
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--refill", type=int, default=0, help="persistent-kernel refill threshold (lanes)")
     return ap.parse_args()
 
 
@@ -237,6 +238,8 @@ def run_ours(args):
     from renderlab_b200 import api as A
     kernel = pick_kernel(args.kernel)
     engine = A.Engine(local)
+    if args.refill:
+        engine.set_tuning(fast_refill=args.refill, wide8_refill=args.refill)
     mesh, words = make_scene(args.triangles)
     scene = engine.upload(A.LAYOUT_REFLECTION, words)
     t_prep = time.perf_counter()

@@ -89,6 +89,13 @@ typedef struct rt_gi_hit {
 /* Any-hit results are one uint32 per ray: 1 when something blocks the ray, else 0
  * (gi_visible returns the negation). */
 
+/* Launch parameters the autotuner chooses (renderlab_b200.tune); zero fields keep defaults. */
+typedef struct rt_tuning {
+  uint32_t fast_refill;  /* FAST: idle lanes (1-32) a persistent warp waits for before taking more rays */
+  uint32_t wide8_refill; /* WIDE8: the same */
+  uint32_t reserved[6];
+} rt_tuning;
+
 typedef struct rt_ctx rt_ctx;
 typedef struct rt_scene rt_scene;
 typedef struct rt_blas rt_blas;
@@ -106,6 +113,8 @@ rt_status rt_ctx_create(int device, rt_ctx** out);
 void rt_ctx_destroy(rt_ctx* ctx);
 const char* rt_get_last_error(const rt_ctx* ctx);
 rt_status rt_get_stats(rt_ctx* ctx, rt_stats* out);
+rt_status rt_ctx_set_tuning(rt_ctx* ctx, const rt_tuning* tuning);
+rt_status rt_ctx_get_tuning(const rt_ctx* ctx, rt_tuning* out);
 /* Runs a small device kernel that reports the device's arithmetic conventions (signed-zero
  * min/max, correctly rounded reciprocal and square root) as 16 result words. */
 rt_status rt_selftest(rt_ctx* ctx, uint32_t out[16]);
@@ -148,6 +157,12 @@ rt_status rt_trace_ex(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kerne
 rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
                         const rt_ray* h_rays, void* h_hits, uint32_t n);
 rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays);
+/* rt_trace_ex in an instrumented build that counts, over the batch, into counts[8]:
+ * rays, top-level nodes, instance box tests, BLAS nodes, leaves, triangles tested, f64
+ * re-tests, f64 final refinements (RT_KERNEL_WIDE8; the bit-exact kernels visit exactly what
+ * the reference traversal visits). Synchronous. */
+rt_status rt_trace_counted(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
+                           const rt_ray* d_rays, void* d_hits, uint32_t n, uint64_t counts[8]);
 
 /* ---- host builders (the CPU side of the path: crates/asset/src/near_field.rs:172-541,
  * src/instance_bvh.rs:162-460, src/gi_bvh.rs, src/reflection_software.rs) ---- */

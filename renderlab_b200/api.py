@@ -54,9 +54,14 @@ class RtInstance(ctypes.Structure):
                 ("extra", ctypes.c_uint32 * 8)]
 
 
+class RtTuning(ctypes.Structure):
+    _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+
+
 EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",
+           "rt_ctx_set_tuning", "rt_ctx_get_tuning",
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
-           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve",
+           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted",
            "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
 
@@ -80,6 +85,8 @@ def lib() -> ctypes.CDLL:
     L.rt_get_last_error.restype = ctypes.c_char_p
     L.rt_get_stats.argtypes = [_vp, ctypes.POINTER(RtStats)]
     L.rt_selftest.argtypes = [_vp, _u32p]
+    L.rt_ctx_set_tuning.argtypes = [_vp, ctypes.POINTER(RtTuning)]
+    L.rt_ctx_get_tuning.argtypes = [_vp, ctypes.POINTER(RtTuning)]
     L.rt_scene_upload.argtypes = [_vp, ctypes.c_int, _u32p, ctypes.c_size_t, ctypes.POINTER(_vp)]
     L.rt_scene_validate.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, _u32p, ctypes.c_char_p, ctypes.c_size_t]
     L.rt_scene_update_records.argtypes = [_vp, _vp, _u32p, ctypes.c_size_t]
@@ -91,6 +98,8 @@ def lib() -> ctypes.CDLL:
     L.rt_trace_ex.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_host.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32]
     L.rt_ctx_reserve.argtypes = [_vp, ctypes.c_uint32]
+    L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
+                                   ctypes.POINTER(ctypes.c_uint64)]
     L.rt_blas_build.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_vp)]
     L.rt_blas_info.argtypes = [_vp, _u32p]
     L.rt_blas_nodes.argtypes = [_vp, _u32p]
@@ -298,6 +307,17 @@ class Engine:
         self._check(lib().rt_selftest(self.ctx, _np_ptr(out, _u32p)))
         return out
 
+    def set_tuning(self, **kw):
+        t = RtTuning()
+        for k, v in kw.items():
+            setattr(t, k, int(v))
+        self._check(lib().rt_ctx_set_tuning(self.ctx, ctypes.byref(t)))
+
+    def tuning(self) -> dict:
+        t = RtTuning()
+        self._check(lib().rt_ctx_get_tuning(self.ctx, ctypes.byref(t)))
+        return {"fast_refill": int(t.fast_refill), "wide8_refill": int(t.wide8_refill)}
+
     def stats(self) -> dict:
         s = RtStats()
         self._check(lib().rt_get_stats(self.ctx, ctypes.byref(s)))
@@ -333,6 +353,19 @@ class Engine:
         hp = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
         self._check(lib().rt_trace_host(self.ctx, scene.handle, mode, KERNELS[kernel], rp, hp, n))
         return out
+
+    COUNTERS = ("rays", "top_nodes", "instance_tests", "nodes", "leaves", "triangles", "f64_retests", "f64_final")
+
+    def trace_counted(self, scene: Scene, rays, mode: int = CLOSEST, kernel: str = "wide8") -> dict:
+        """Trace in the instrumented build; returns the visit counters over the batch."""
+        import torch
+        n = rays.shape[0]
+        words = hit_words(scene.layout, mode)
+        hits = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=rays.device)
+        out = (ctypes.c_uint64 * 8)()
+        self._check(lib().rt_trace_counted(self.ctx, scene.handle, mode, KERNELS[kernel], rays.data_ptr(),
+                                           hits.data_ptr(), n, out))
+        return dict(zip(self.COUNTERS, map(int, out)))
 
     def reserve(self, max_rays: int):
         self._check(lib().rt_ctx_reserve(self.ctx, max_rays))

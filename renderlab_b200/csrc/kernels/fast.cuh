@@ -24,12 +24,14 @@ RT_DEV float byte_f(uint32_t word, uint32_t shift) {
 struct RayQueue {
   unsigned int* next;  // global counter, zeroed before the launch
   uint32_t n;
+  uint32_t refill;     // idle lanes a warp waits for before taking more rays (1-32)
 };
 
 // Called by all 32 lanes together. `drained` (warp-uniform) stops the requests once the
 // counter has passed the end, so finished warps add no atomic traffic.
 RT_DEV uint32_t take_ray(const RayQueue& q, bool need, bool& drained) {
-  const unsigned want = __ballot_sync(0xffffffffu, need && !drained);
+  const unsigned idle = __ballot_sync(0xffffffffu, need);
+  const unsigned want = (!drained && (uint32_t)__popc(idle) >= q.refill) ? idle : 0u;
   if (!want) return EMPTY;
   const int lane = threadIdx.x & 31;
   const int leader = __ffs(want) - 1;

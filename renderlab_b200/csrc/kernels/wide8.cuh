@@ -25,6 +25,13 @@ constexpr float W8_TIE = 8e-6f;
 constexpr float W8_EDGE = 1e-5f;
 constexpr uint32_t W8_STACK = 32;
 
+// Opt-in device counters of the WIDE8 walk (diagnostics and the bytes-per-ray roofline).
+enum W8Count { W8C_RAYS, W8C_TOP_NODES, W8C_INSTANCE_TESTS, W8C_NODES, W8C_LEAVES, W8C_TRIS, W8C_RETESTS, W8C_FINAL64, W8C_N };
+template <bool COUNT>
+RT_DEV void w8_count(unsigned long long* cnt, int k, unsigned long long n = 1) {
+  if (COUNT) atomicAdd(cnt + k, n);
+}
+
 struct W8View {
   const uint4* nodes;     // 5 uint4 a node
   const uint4* tris;      // 3 uint4 a triangle
@@ -191,9 +198,10 @@ RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, 
 }
 
 // Considers one candidate triangle; returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, bool ANY>
+template <uint32_t LAYOUT, bool ANY, bool COUNT>
 RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const W8Ray& R, const Ray& ray, uint32_t inst,
-                         uint32_t tri, W8Best& best) {
+                         uint32_t tri, W8Best& best, unsigned long long* cnt) {
+  w8_count<COUNT>(cnt, W8C_TRIS);
   const uint4 q0 = __ldg(V.tris + 3 * (size_t)tri), q1 = __ldg(V.tris + 3 * (size_t)tri + 1),
               q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
   const F3 v0 = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
@@ -219,6 +227,7 @@ RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const 
                          (best.hit && t >= best.t - band - best.band);
   double t64 = 0.0, u64 = 0.0, v64 = 0.0;
   if (uncertain) {
+    w8_count<COUNT>(cnt, W8C_RETESTS);
     if (!mt64<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) return false;
     if (best.hit && !best.has64) {
       // the incumbent needs its f64 result too
@@ -272,8 +281,10 @@ struct W8Lane {
 
 // One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
 // Returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, bool ANY>
-RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st) {
+template <uint32_t LAYOUT, bool ANY, bool COUNT>
+RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st,
+                    unsigned long long* cnt) {
+  w8_count<COUNT>(cnt, W8C_NODES);
   const W8Ray& R = L.R;
   const uint4* np = V.nodes + 5 * (size_t)L.node;
   const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
@@ -326,8 +337,9 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
     leaf_hits &= leaf_hits - 1;
     const uint32_t m = ((s < 4 ? meta_lo : meta_hi) >> (8 * (s & 3))) & 0xffu;
     const uint32_t first = tri_base + (m & 31u), count = m >> 5;
+    w8_count<COUNT>(cnt, W8C_LEAVES);
     for (uint32_t k = 0; k < count; ++k)
-      if (w8_candidate<LAYOUT, ANY>(w, V, R, L.ray, L.inst, first + k, L.best)) return true;
+      if (w8_candidate<LAYOUT, ANY, COUNT>(w, V, R, L.ray, L.inst, first + k, L.best, cnt)) return true;
   }
   const uint32_t inner = oct_permute(hits & imask, R.oct);
   if (inner) {
@@ -356,8 +368,8 @@ RT_DEV bool w8_next(W8Lane& L, const uint2* stack) {
 }
 
 // Enters instance i when its world box survives; sets up the object-space ray.
-template <uint32_t LAYOUT, bool ANY>
-RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i) {
+template <uint32_t LAYOUT, bool ANY, bool COUNT>
+RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i, unsigned long long* cnt) {
   const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;
   if (ANY && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
   const W8Best& best = L.best;
@@ -379,8 +391,10 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   L.phase = 2;
 }
 
-template <uint32_t LAYOUT, bool ANY>
-RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, void* __restrict__ out) {
+template <uint32_t LAYOUT, bool ANY, bool COUNT>
+RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, void* __restrict__ out,
+                      unsigned long long* cnt) {
+  w8_count<COUNT>(cnt, W8C_RAYS);
   W8Best& b = L.best;
   const uint32_t id = L.ray_id;
   L.phase = 0;
@@ -389,6 +403,7 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
     return;
   }
   if (b.hit && !b.has64 && b.abs_err > 2e-6f * b.t) {
+    w8_count<COUNT>(cnt, W8C_FINAL64);
     // the f32 t is not within 1e-5 relative: report the f64 one
     const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(V.tris) + 12 * (size_t)b.tri + 10);
     double t64, u64, v64;
@@ -430,10 +445,11 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
 // Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
 // step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
 // re-converges at the top of the loop.
-template <uint32_t LAYOUT, bool ANY, int BLOCK>
+template <uint32_t LAYOUT, bool ANY, int BLOCK, bool COUNT>
 __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__ w, W8View V, const float4* __restrict__ rays,
                                                  const uint32_t* __restrict__ order, void* __restrict__ out,
-                                                 unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
+                                                 unsigned int* __restrict__ counter, uint32_t n, DevStatus* st,
+                                                 unsigned long long* cnt, uint32_t refill) {
   uint2 stack[W8_STACK];
   uint32_t tstack[STACK];
   W8Lane L;
@@ -443,8 +459,10 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__
   bool drained = false;
   for (;;) {
     __syncwarp();
-    // ray refill (warp-aggregated)
-    const unsigned want = __ballot_sync(0xffffffffu, L.phase == 0 && !drained);
+    // ray refill (warp-aggregated) once `refill` lanes are idle: 1 keeps every lane busy,
+    // 32 hands out whole runs of 32 consecutive rays (keeps a coherent batch's tiles together)
+    const unsigned idle = __ballot_sync(0xffffffffu, L.phase == 0);
+    const unsigned want = (!drained && (uint32_t)__popc(idle) >= refill) ? idle : 0u;
     uint32_t id = EMPTY;
     if (want) {
       const int lane = threadIdx.x & 31, leader = __ffs(want) - 1;
@@ -475,30 +493,31 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__
       if (L.node == EMPTY && !w8_next(L, stack)) {
         L.phase = 1;
       } else {
-        if (w8_node<LAYOUT, ANY>(w, V, L, stack, st)) w8_finish<LAYOUT, ANY>(w, V, L, out);
+        if (w8_node<LAYOUT, ANY, COUNT>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, ANY, COUNT>(w, V, L, out, cnt);
         continue;
       }
     }
     if (L.phase == 1) {
       if (top == 0) {
         if (L.flat >= count) {
-          w8_finish<LAYOUT, ANY>(w, V, L, out);
+          w8_finish<LAYOUT, ANY, COUNT>(w, V, L, out, cnt);
           continue;
         }
-        w8_enter<LAYOUT, ANY>(w, V, L, L.flat++);
+        w8_enter<LAYOUT, ANY, COUNT>(w, V, L, L.flat++, cnt);
         continue;
       }
       if (L.tsp == 0) {
-        w8_finish<LAYOUT, ANY>(w, V, L, out);
+        w8_finish<LAYOUT, ANY, COUNT>(w, V, L, out, cnt);
         continue;
       }
       const uint32_t item = tstack[--L.tsp];
       if (item & LEAF) {
-        w8_enter<LAYOUT, ANY>(w, V, L, item & ~LEAF);
+        w8_enter<LAYOUT, ANY, COUNT>(w, V, L, item & ~LEAF, cnt);
         continue;
       }
       const W8Best& b = L.best;
       const float bound = b.hit ? b.t + 2.0f * b.band + 2.0f * W8_TIE * b.t : b.t;
+      w8_count<COUNT>(cnt, W8C_TOP_NODES);
       top_step(w, top_base + (size_t)item * 32, L.ray, L.world_inv, bound, tstack, L.tsp, st);
     }
   }

@@ -38,25 +38,25 @@ cudaError_t grid_for(K kernel, uint32_t n, dim3& grid) {
 
 template <class K>
 cudaError_t run(K kernel, const SceneView& s, const float4* rays, const uint32_t* order, void* hits, uint32_t n,
-                unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+                unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
   dim3 grid;
   cudaError_t e = grid_for(kernel, n, grid);
   if (e != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-  kernel<<<grid, FAST_BLOCK, 0, stream>>>(s.words, rays, order, hits, rtk::RayQueue{counter, n}, st);
+  kernel<<<grid, FAST_BLOCK, 0, stream>>>(s.words, rays, order, hits, rtk::RayQueue{counter, n, refill}, st);
   return cudaGetLastError();
 }
 }  // namespace
 
 cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
   if (n == 0) return cudaSuccess;
   if (s.layout == 0) {
-    if (mode == 0) return run(rtk::k_gi_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
-    return run(rtk::k_gi_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
+    if (mode == 0) return run(rtk::k_gi_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
+    return run(rtk::k_gi_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
   }
-  if (mode == 0) return run(rtk::k_rs_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
-  return run(rtk::k_rs_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream);
+  if (mode == 0) return run(rtk::k_rs_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
+  return run(rtk::k_rs_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
 }
 
 }  // namespace rtl

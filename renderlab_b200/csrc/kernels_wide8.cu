@@ -25,18 +25,21 @@ cudaError_t resident(K kernel, uint32_t& out) {
 
 template <class K>
 cudaError_t run(K kernel, const uint32_t* words, const rtk::W8View& v, const float4* rays, const uint32_t* order,
-                void* hits, unsigned int* counter, uint32_t n, rtk::DevStatus* st, cudaStream_t stream) {
+                void* hits, unsigned int* counter, uint32_t n, rtk::DevStatus* st, cudaStream_t stream,
+                unsigned long long* cnt, uint32_t refill) {
   uint32_t full = 0;
   cudaError_t e = resident(kernel, full);
   if (e != cudaSuccess) return e;
   const uint32_t need = (n + W8_BLOCK - 1) / W8_BLOCK;
   if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-  kernel<<<need < full ? need : full, W8_BLOCK, 0, stream>>>(words, v, rays, order, hits, counter, n, st);
+  kernel<<<need < full ? need : full, W8_BLOCK, 0, stream>>>(words, v, rays, order, hits, counter, n, st, cnt, refill);
   return cudaGetLastError();
 }
 
-cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+template <bool COUNT>
+cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
+                       uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
+                       unsigned long long* cnt, uint32_t refill) {
   if (n == 0) return cudaSuccess;
   if (!s.wide8) return cudaErrorInvalidValue;
   rtk::W8View v;
@@ -45,11 +48,21 @@ cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, 
   v.tris = reinterpret_cast<const uint4*>(base + s.w8_tris_at);
   v.inst = base + s.w8_inst_at;
   if (s.layout == 0) {
-    if (mode == 0) return run(rtk::k_wide8<0, false, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
-    return run(rtk::k_wide8<0, true, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
+    if (mode == 0) return run(rtk::k_wide8<0, false, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
+    return run(rtk::k_wide8<0, true, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
   }
-  if (mode == 0) return run(rtk::k_wide8<1, false, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
-  return run(rtk::k_wide8<1, true, W8_BLOCK>, s.words, v, rays, order, hits, counter, n, st, stream);
+  if (mode == 0) return run(rtk::k_wide8<1, false, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
+  return run(rtk::k_wide8<1, true, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
+}
+
+cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
+                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
+  return launch_any<false>(s, mode, rays, order, hits, n, counter, st, stream, nullptr, refill);
+}
+
+cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
+                        unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream) {
+  return launch_any<true>(s, mode, rays, nullptr, hits, n, counter, st, stream, cnt, 1);
 }
 
 }  // namespace rtl

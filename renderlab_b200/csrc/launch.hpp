@@ -27,10 +27,14 @@ cudaError_t launch_plain(const SceneView& s, uint32_t mode, const float4* rays, 
 // FAST: bit-exact with PLAIN; `order` (optional) permutes which ray each thread traces.
 // `counter` is a device word the launch owns until it completes (zeroed on `stream`).
 cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream);
+                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
 // WIDE8: the precision variant over the scene's derived 8-wide layout.
+// `refill`: idle lanes (1-32) a warp waits for before it takes more rays.
 cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream);
+                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
+// WIDE8 with per-event device counters (rtk::W8Count order) accumulated into cnt[8].
+cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
+                        unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream);
 cudaError_t launch_selftest(uint32_t* out16, cudaStream_t stream);
 
 }  // namespace rtl

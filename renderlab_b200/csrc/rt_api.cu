@@ -39,6 +39,7 @@ struct rt_ctx {
   // many launches may be in flight at once across streams.
   unsigned int* d_counters = nullptr;
   std::atomic<uint64_t> counter_seq{0};
+  rt_tuning tuning = {1, 1, {0, 0, 0, 0, 0, 0}};
   std::mutex mu;
   std::string last_error;
   std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
@@ -103,13 +104,15 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
       break;
     case RT_KERNEL_FAST:
       e = rtl::launch_fast(v, (uint32_t)mode, r, order, hits, n,
-                           ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream);
+                           ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream,
+                           ctx->tuning.fast_refill);
       break;
     case RT_KERNEL_WIDE8:
       if (!scene->d_wide8)
         return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
       e = rtl::launch_wide8(v, (uint32_t)mode, r, order, hits, n,
-                            ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream);
+                            ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream,
+                            ctx->tuning.wide8_refill);
       break;
     default:
       return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
@@ -175,6 +178,23 @@ rt_status rt_get_stats(rt_ctx* ctx, rt_stats* out) {
   out->stack_overflows = st.stack_drops;
   out->launches = ctx->launches;
   out->scene_bytes = ctx->scene_bytes;
+  return RT_OK;
+}
+
+rt_status rt_ctx_set_tuning(rt_ctx* ctx, const rt_tuning* t) {
+  if (!ctx || !t) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  rt_tuning next = ctx->tuning;
+  for (uint32_t v : {t->fast_refill, t->wide8_refill})
+    if (v > 32) return fail(ctx, RT_ERR_INVALID_ARG, "refill thresholds are 1-32 lanes");
+  if (t->fast_refill) next.fast_refill = t->fast_refill;
+  if (t->wide8_refill) next.wide8_refill = t->wide8_refill;
+  ctx->tuning = next;
+  return RT_OK;
+}
+
+rt_status rt_ctx_get_tuning(const rt_ctx* ctx, rt_tuning* out) {
+  if (!ctx || !out) return RT_ERR_INVALID_ARG;
+  *out = ctx->tuning;
   return RT_OK;
 }
 
@@ -310,6 +330,27 @@ rt_status rt_trace_ex(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kerne
   if (reinterpret_cast<uintptr_t>(d_rays) % 16 != 0) return fail(ctx, RT_ERR_INVALID_ARG, "rays must be 16-byte aligned");
   if (reinterpret_cast<uintptr_t>(d_hits) % 4 != 0) return fail(ctx, RT_ERR_INVALID_ARG, "hits must be 4-byte aligned");
   return dispatch(ctx, scene, mode, kernel, d_rays, d_order, d_hits, n, static_cast<cudaStream_t>(stream));
+}
+
+rt_status rt_trace_counted(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* d_rays,
+                           void* d_hits, uint32_t n, uint64_t counts[8]) {
+  rt_status s = check_trace_args(ctx, scene, mode, kernel);
+  if (s != RT_OK) return s;
+  if (!d_rays || !d_hits || !counts) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if (kernel != RT_KERNEL_WIDE8) return fail(ctx, RT_ERR_UNSUPPORTED, "counted traversal is provided for RT_KERNEL_WIDE8");
+  if (!scene->d_wide8) return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare first");
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  unsigned long long* d_cnt = nullptr;
+  RT_CUDA(ctx, cudaMalloc(&d_cnt, 8 * sizeof(unsigned long long)));
+  cudaError_t e = cudaMemset(d_cnt, 0, 8 * sizeof(unsigned long long));
+  if (e == cudaSuccess)
+    e = rtl::count_wide8(view_of(scene), (uint32_t)mode, reinterpret_cast<const float4*>(d_rays), d_hits, n,
+                         ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, d_cnt, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(counts, d_cnt, 8 * sizeof(unsigned long long), cudaMemcpyDeviceToHost);
+  cudaFree(d_cnt);
+  if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "counted traversal: %s", cudaGetErrorString(e));
+  return RT_OK;
 }
 
 rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays) {
