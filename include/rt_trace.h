@@ -164,6 +164,21 @@ rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays);
 rt_status rt_trace_counted(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
                            const rt_ray* d_rays, void* d_hits, uint32_t n, uint64_t counts[8]);
 
+/* ---- allocation-free traversal ----
+ * No counterpart in the reference: renderlab always traverses inside its own renderer.
+ * rt_trace_static is the FAST traversal for a caller that cannot allocate device memory -- an
+ * engine whose frame loop forbids cudaMalloc, or one that keeps the packed words in its own
+ * device buffer and creates no rt_ctx. It allocates nothing: the kernel's scratch (its ray
+ * counter and overflow count) is a static 256-byte device array that each GPU loading the
+ * library holds until exit. d_words must be words rt_scene_validate accepted, copied to the
+ * device by the caller (16-byte aligned); n is at most RT_STATIC_MAX_RAYS, larger batches are
+ * refused with RT_ERR_INVALID_ARG. Hits are written as rt_trace writes them. The first call on
+ * a device looks up the array's device address; make it before any stream capture. Every call
+ * reuses (and first zeroes) the same array, so calls that overlap on the GPU race. */
+#define RT_STATIC_MAX_RAYS (1u << 31)
+rt_status rt_trace_static(rt_layout layout, const uint32_t* d_words, size_t n_words, rt_mode mode,
+                          const rt_ray* d_rays, void* d_hits, uint32_t n, void* stream);
+
 /* ---- host builders (the CPU side of the path: crates/asset/src/near_field.rs:172-541,
  * src/instance_bvh.rs:162-460, src/gi_bvh.rs, src/reflection_software.rs) ---- */
 #define RT_BUILD_SAH 0u    /* build_bvh_sah (near_field.rs:184): binned SAH, median past depth 15 */

@@ -62,7 +62,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_ctx_set_tuning", "rt_ctx_get_tuning",
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted",
-           "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
+           "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
 
 _lib = None
@@ -98,6 +98,7 @@ def lib() -> ctypes.CDLL:
     L.rt_trace_ex.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_host.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32]
     L.rt_ctx_reserve.argtypes = [_vp, ctypes.c_uint32]
+    L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
     L.rt_blas_build.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_vp)]
@@ -369,6 +370,26 @@ class Engine:
 
     def reserve(self, max_rays: int):
         self._check(lib().rt_ctx_reserve(self.ctx, max_rays))
+
+
+STATIC_MAX_RAYS = 1 << 31
+
+
+def trace_static(layout: int, d_words, rays, mode: int = CLOSEST, hits=None, stream=None):
+    """rt_trace_static: the FAST traversal with no allocation by the library and no context.
+
+    d_words: the packed words in a caller-owned torch CUDA tensor (int32/uint32 view, words that
+    `validate` accepted); rays: (n, 8) float32 CUDA tensor. Returns the int32 hit tensor."""
+    import torch
+    n = rays.shape[0]
+    words = hit_words(layout, mode)
+    if hits is None:
+        hits = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=rays.device)
+    s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+    st = lib().rt_trace_static(layout, d_words.data_ptr(), d_words.numel(), mode, rays.data_ptr(), hits.data_ptr(), n, s)
+    if st != 0:
+        raise RtError(st, "rt_trace_static refused the call (sizes, alignment or layout)")
+    return hits
 
 
 # ---------------------------------------------------------------- the seam, batched
