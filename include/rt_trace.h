@@ -151,6 +151,18 @@ rt_status rt_trace(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, const rt_ra
 rt_status rt_trace_ex(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
                       const rt_ray* d_rays, const uint32_t* d_order, void* d_hits, uint32_t n,
                       void* stream);
+/* Ray order keys for rt_order_rays. */
+typedef enum rt_ray_order {
+  RT_ORDER_NONE = 0,
+  RT_ORDER_ORIGIN = 1,            /* Morton code of the origin in the scene's bounds */
+  RT_ORDER_OCTANT_ORIGIN = 2,     /* direction octant, then the origin's Morton code */
+  RT_ORDER_DIRECTION_ORIGIN = 3   /* octahedral direction cell, then a coarse origin code */
+} rt_ray_order;
+/* Writes to d_order (n uint32) a permutation of the rays that groups nearby, alike rays, for
+ * rt_trace_ex. Uses the context's ordering scratch (allocated on first use, or sized ahead by
+ * rt_ctx_reserve). Asynchronous on `stream`. */
+rt_status rt_order_rays(rt_ctx* ctx, const rt_scene* scene, const rt_ray* d_rays, uint32_t n, rt_ray_order key,
+                        uint32_t* d_order, void* stream);
 /* Host-buffer form: copies rays in and hits out through the context's pinned staging and
  * device buffers (grown on first use, or sized ahead by rt_ctx_reserve), pipelined in chunks
  * over two streams. Returns when the hits are in h_hits. */

@@ -27,6 +27,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "librt_trace.so"
 LAYOUT_GI, LAYOUT_REFLECTION = 0, 1
 CLOSEST, ANY_SKY, ANY_CASTERS = 0, 1, 2
 KERNELS = {"plain": 0, "fast": 1, "wide8": 2}
+ORDERS = {"none": 0, "origin": 1, "octant": 2, "direction": 3}
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "LAYOUT", 3: "OOM", 4: "STACK_OVERFLOW", 5: "TIMEOUT",
           6: "CUDA", 7: "BUSY", 8: "UNSUPPORTED"}
 GI_HIT_WORDS, RS_HIT_WORDS = 10, 5
@@ -61,7 +62,7 @@ class RtTuning(ctypes.Structure):
 EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",
            "rt_ctx_set_tuning", "rt_ctx_get_tuning",
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
-           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted",
+           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
 
@@ -98,6 +99,7 @@ def lib() -> ctypes.CDLL:
     L.rt_trace_ex.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_host.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32]
     L.rt_ctx_reserve.argtypes = [_vp, ctypes.c_uint32]
+    L.rt_order_rays.argtypes = [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int, _vp, _vp]
     L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
@@ -317,7 +319,7 @@ class Engine:
     def tuning(self) -> dict:
         t = RtTuning()
         self._check(lib().rt_ctx_get_tuning(self.ctx, ctypes.byref(t)))
-        return {"fast_refill": int(t.fast_refill), "wide8_refill": int(t.wide8_refill)}
+        return {f: int(getattr(t, f)) for f, _ in RtTuning._fields_ if f != "reserved"}
 
     def stats(self) -> dict:
         s = RtStats()
@@ -353,6 +355,16 @@ class Engine:
         rp = rays.data_ptr() if hasattr(rays, "data_ptr") else rays.ctypes.data
         hp = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
         self._check(lib().rt_trace_host(self.ctx, scene.handle, mode, KERNELS[kernel], rp, hp, n))
+        return out
+
+    def order(self, scene: Scene, rays, key: str = "octant", out=None, stream=None):
+        """A permutation of `rays` (CUDA tensor) grouping alike rays; int32 CUDA tensor."""
+        import torch
+        n = rays.shape[0]
+        if out is None:
+            out = torch.empty(n, dtype=torch.int32, device=rays.device)
+        s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+        self._check(lib().rt_order_rays(self.ctx, scene.handle, rays.data_ptr(), n, ORDERS[key], out.data_ptr(), s))
         return out
 
     COUNTERS = ("rays", "top_nodes", "instance_tests", "nodes", "leaves", "triangles", "f64_retests", "f64_final")

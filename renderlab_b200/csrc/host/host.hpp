@@ -92,6 +92,7 @@ struct SceneInfo {
   size_t nodes = 0;           // distinct BLAS nodes
   uint32_t max_blas_depth = 0;
   uint32_t max_top_depth = 0;
+  Aabb world = Aabb::empty();  // union of the instance world boxes
 };
 bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& info, std::string& err);
 

@@ -88,6 +88,10 @@ bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& inf
       std::map<std::array<uint32_t, 6>, bool> done;
       for (uint32_t i = 0; i < count; ++i) {
         const uint32_t* r = w + 16 + 32 * (size_t)i;
+        for (int a = 0; a < 3; ++a) {
+          info.world.lo[a] = lo_of(info.world.lo[a], as_float(r[12 + a]));
+          info.world.hi[a] = hi_of(info.world.hi[a], as_float(r[15 + a]));
+        }
         std::array<uint32_t, 6> key = {r[18], r[19], r[20], r[21], r[22], r[28]};
         if (done.count(key)) continue;
         done[key] = true;
@@ -126,6 +130,10 @@ bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& inf
       std::map<std::array<uint32_t, 6>, bool> done;
       for (uint32_t i = 0; i < count; ++i) {
         const uint32_t* r = w + 8 + 24 * (size_t)i;
+        for (int a = 0; a < 3; ++a) {
+          info.world.lo[a] = lo_of(info.world.lo[a], as_float(r[12 + a]));
+          info.world.hi[a] = hi_of(info.world.hi[a], as_float(r[15 + a]));
+        }
         std::array<uint32_t, 6> key = {r[18] & ~3u, r[19] & ~3u, r[20], 0, 0, 0};
         if (done.count(key)) continue;
         done[key] = true;

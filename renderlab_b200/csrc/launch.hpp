@@ -35,6 +35,11 @@ cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, 
 // WIDE8 with per-event device counters (rtk::W8Count order) accumulated into cnt[8].
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream);
+// Ray ordering (kernels_order.cu): scratch holds the keys, the unsorted indices and the radix
+// sort's temporary storage.
+size_t order_scratch_bytes(uint32_t n);
+cudaError_t launch_order(const float4* rays, uint32_t n, const float lo[3], const float hi[3], uint32_t kind,
+                         uint32_t* order, void* scratch, size_t scratch_bytes, cudaStream_t stream);
 cudaError_t launch_selftest(uint32_t* out16, cudaStream_t stream);
 
 }  // namespace rtl

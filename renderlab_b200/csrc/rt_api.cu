@@ -3,6 +3,7 @@
 
 #include <algorithm>
 #include <atomic>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <memory>
@@ -39,7 +40,7 @@ struct rt_ctx {
   // many launches may be in flight at once across streams.
   unsigned int* d_counters = nullptr;
   std::atomic<uint64_t> counter_seq{0};
-  rt_tuning tuning = {1, 1, {0, 0, 0, 0, 0, 0}};
+  rt_tuning tuning = {8, 8, {0, 0, 0, 0, 0, 0}};
   std::mutex mu;
   std::string last_error;
   std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
@@ -48,6 +49,9 @@ struct rt_ctx {
   void* d_rays = nullptr;
   void* d_hits = nullptr;
   size_t stage_rays = 0;  // rays per chunk buffer
+  // rt_order_rays scratch
+  void* d_order_scratch = nullptr;
+  size_t order_scratch_bytes = 0;
 };
 
 namespace {
@@ -164,6 +168,7 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   cudaFree(ctx->d_counters);
   cudaFree(ctx->d_rays);
   cudaFree(ctx->d_hits);
+  cudaFree(ctx->d_order_scratch);
   delete ctx;
 }
 
@@ -353,9 +358,53 @@ rt_status rt_trace_counted(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_
   return RT_OK;
 }
 
+namespace {
+// Grows the ordering scratch to cover n rays (caller holds ctx->mu).
+rt_status ensure_order_scratch(rt_ctx* ctx, uint32_t n) {
+  const size_t need = rtl::order_scratch_bytes(n);
+  if (need <= ctx->order_scratch_bytes) return RT_OK;
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, cudaDeviceSynchronize());
+  cudaFree(ctx->d_order_scratch);
+  ctx->d_order_scratch = nullptr;
+  ctx->order_scratch_bytes = 0;
+  if (cudaMalloc(&ctx->d_order_scratch, need) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RT_ERR_OOM, "ordering scratch of %zu bytes", need);
+  }
+  ctx->order_scratch_bytes = need;
+  return RT_OK;
+}
+}  // namespace
+
+rt_status rt_order_rays(rt_ctx* ctx, const rt_scene* scene, const rt_ray* d_rays, uint32_t n, rt_ray_order key,
+                        uint32_t* d_order, void* stream) {
+  if (!ctx || !scene || (n && (!d_rays || !d_order))) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if ((unsigned)key > 3u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown ray order %d", (int)key);
+  if (n == 0) return RT_OK;
+  std::lock_guard<std::mutex> lock(ctx->mu);
+  rt_status s = ensure_order_scratch(ctx, n);
+  if (s != RT_OK) return s;
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const rtb::Aabb& wb = scene->info.world;
+  float lo[3], hi[3];
+  for (int a = 0; a < 3; ++a) {
+    lo[a] = std::isfinite(wb.lo[a]) ? wb.lo[a] : -1.0f;
+    hi[a] = std::isfinite(wb.hi[a]) ? wb.hi[a] : 1.0f;
+  }
+  if (key == RT_ORDER_NONE) key = RT_ORDER_ORIGIN;
+  RT_CUDA(ctx, rtl::launch_order(reinterpret_cast<const float4*>(d_rays), n, lo, hi, (uint32_t)key, d_order,
+                                 ctx->d_order_scratch, ctx->order_scratch_bytes, static_cast<cudaStream_t>(stream)));
+  return RT_OK;
+}
+
 rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays) {
   if (!ctx) return RT_ERR_INVALID_ARG;
   std::lock_guard<std::mutex> lock(ctx->mu);
+  {
+    rt_status so = ensure_order_scratch(ctx, max_rays);
+    if (so != RT_OK) return so;
+  }
   const size_t want = std::min<size_t>(max_rays, HOST_CHUNK);
   if (want <= ctx->stage_rays) return RT_OK;
   RT_CUDA(ctx, cudaSetDevice(ctx->device));

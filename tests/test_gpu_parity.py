@@ -279,3 +279,36 @@ def deep_chain_scene(depth: int) -> np.ndarray:
     head[4] = 8 + 24 + 32
     bounds = np.array([-1, -1, -1, 0, 2, 2, 1, 0], np.float32).view(np.uint32)
     return np.concatenate([head, rec, np.zeros(32, np.uint32), bounds, node_words, tris.reshape(-1)]).astype(np.uint32)
+
+
+@pytest.mark.parametrize("key", ["origin", "octant", "direction"])
+def test_ray_order_is_a_permutation_and_changes_no_result(engine, key):
+    """rt_order_rays returns a permutation of the batch; tracing through it (FAST and WIDE8) gives
+    every ray the same result as tracing in the given order."""
+    torch = _torch()
+    mesh, rays = H.small_clusters()
+    w = product_words(A.LAYOUT_REFLECTION, [mesh], S.identity_instances(1))
+    scene = engine.upload(A.LAYOUT_REFLECTION, w)
+    try:
+        want, _ = O.rs_trace(w, rays, False)
+        hit = want[:, 1] != 0
+        pts = S.hit_points(rays[hit], want[hit, 0].view(np.float32))
+        gi = S.hemisphere_rays(pts, S.triangle_normals(mesh, want[hit, 2]), rays[hit, 4:7], 30_000, S.Stream(7))
+        batch = np.concatenate([rays, gi])
+        d = torch.from_numpy(batch).cuda()
+        order = engine.order(scene, d, key)
+        torch.cuda.synchronize()
+        perm = order.cpu().numpy()
+        assert np.array_equal(np.sort(perm), np.arange(len(batch)))
+        assert not np.array_equal(perm, np.arange(len(batch)))
+        scene.prepare("wide8")
+        for kernel in ("fast", "wide8"):
+            plain = engine.trace(scene, d, A.CLOSEST, kernel)
+            sorted_ = engine.trace(scene, d, A.CLOSEST, kernel, order=order)
+            torch.cuda.synchronize()
+            assert torch.equal(plain, sorted_), kernel
+        got = engine.trace(scene, d, A.CLOSEST, "fast", order=order).cpu().numpy().view(np.uint32)
+        want_all, _ = O.rs_trace(w, batch, False)
+        check_same(got, want_all, "ordered fast")
+    finally:
+        scene.release()
