@@ -163,6 +163,42 @@ typedef enum rt_ray_order {
  * rt_ctx_reserve). Asynchronous on `stream`. */
 rt_status rt_order_rays(rt_ctx* ctx, const rt_scene* scene, const rt_ray* d_rays, uint32_t n, rt_ray_order key,
                         uint32_t* d_order, void* stream);
+/* ---- Many batches in one launch ----------------------------------------------------------
+ * Uneven ray batches of one scene, each with its own buffers and mode, traced by ONE persistent
+ * launch that hands out rays from the concatenation of the batches. Per batch, the results are
+ * exactly those rt_trace_ex would write for it alone with the same kernel. No counterpart in the
+ * reference (its passes dispatch one compute shader per ray buffer). */
+typedef struct rt_batch {
+  const rt_ray* d_rays; /* device rays */
+  void* d_hits;         /* device results: as rt_trace for this batch's mode */
+  uint32_t n;
+  rt_mode mode;
+} rt_batch;
+#define RT_MAX_BATCHES 4096u
+/* Stream-ordered; the batch table is staged through the context (h_batches may be reused on
+ * return). kernel: RT_KERNEL_FAST or RT_KERNEL_WIDE8. At most RT_MAX_BATCHES batches. */
+rt_status rt_trace_batches(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const rt_batch* h_batches,
+                           uint32_t n_batches, void* stream);
+
+/* A prepared many-batch launch: its batch table resident on the device, an optional ray sort, and
+ * the whole launch captured once in a CUDA graph and replayed by rt_plan_launch. The batches'
+ * buffers must stay valid for the plan's life; their contents may change between launches (the
+ * plan re-sorts on every launch). Launches of one plan must not overlap (they share its ray
+ * counter): issue them on one stream. */
+typedef struct rt_plan rt_plan;
+typedef struct rt_plan_desc {
+  rt_kernel kernel;   /* RT_KERNEL_FAST or RT_KERNEL_WIDE8 */
+  uint32_t refill;    /* idle lanes (1-32) before a warp takes more rays; 0: the context's tuning */
+  rt_ray_order order; /* sort the launch's rays first (RT_ORDER_NONE: no sort) */
+  uint32_t graph;     /* 1: replay a captured CUDA graph; 0: launch directly */
+} rt_plan_desc;
+rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_batches, uint32_t n_batches,
+                         const rt_plan_desc* desc, rt_plan** out);
+rt_status rt_plan_launch(rt_plan* plan, void* stream);
+/* Rays the plan traces per launch and device bytes it holds (table, counter, sort scratch). */
+rt_status rt_plan_info(const rt_plan* plan, uint64_t* rays, uint64_t* device_bytes);
+rt_status rt_plan_destroy(rt_plan* plan);
+
 /* Host-buffer form: copies rays in and hits out through the context's pinned staging and
  * device buffers (grown on first use, or sized ahead by rt_ctx_reserve), pipelined in chunks
  * over two streams. Returns when the hits are in h_hits. */

@@ -55,6 +55,14 @@ class RtInstance(ctypes.Structure):
                 ("extra", ctypes.c_uint32 * 8)]
 
 
+class RtBatch(ctypes.Structure):
+    _fields_ = [("d_rays", ctypes.c_void_p), ("d_hits", ctypes.c_void_p), ("n", ctypes.c_uint32), ("mode", ctypes.c_int)]
+
+
+class RtPlanDesc(ctypes.Structure):
+    _fields_ = [("kernel", ctypes.c_int), ("refill", ctypes.c_uint32), ("order", ctypes.c_int), ("graph", ctypes.c_uint32)]
+
+
 class RtTuning(ctypes.Structure):
     _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
@@ -63,6 +71,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_ctx_set_tuning", "rt_ctx_get_tuning",
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
+           "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
 
@@ -100,6 +109,12 @@ def lib() -> ctypes.CDLL:
     L.rt_trace_host.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32]
     L.rt_ctx_reserve.argtypes = [_vp, ctypes.c_uint32]
     L.rt_order_rays.argtypes = [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int, _vp, _vp]
+    L.rt_trace_batches.argtypes = [_vp, _vp, ctypes.c_int, ctypes.POINTER(RtBatch), ctypes.c_uint32, _vp]
+    L.rt_plan_create.argtypes = [_vp, _vp, ctypes.POINTER(RtBatch), ctypes.c_uint32, ctypes.POINTER(RtPlanDesc),
+                                 ctypes.POINTER(_vp)]
+    L.rt_plan_launch.argtypes = [_vp, _vp]
+    L.rt_plan_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
+    L.rt_plan_destroy.argtypes = [_vp]
     L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
@@ -281,6 +296,35 @@ class Scene:
         return int(lib().rt_scene_device_bytes(self.handle))
 
 
+class Plan:
+    """A many-batch launch prepared once and replayed (a CUDA graph unless graph=False). Holds
+    the batches' ray tensors and owns their hit tensors (`hits`)."""
+
+    def __init__(self, engine: "Engine", scene: Scene, handle, hits, rays, desc: dict):
+        self.engine, self.scene, self.handle, self.hits, self.rays, self.desc = engine, scene, handle, hits, rays, desc
+
+    def launch(self, stream=None):
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self.engine._check(lib().rt_plan_launch(self.handle, s))
+
+    def info(self) -> dict:
+        rays, nbytes = ctypes.c_uint64(), ctypes.c_uint64()
+        self.engine._check(lib().rt_plan_info(self.handle, ctypes.byref(rays), ctypes.byref(nbytes)))
+        return {"rays": int(rays.value), "device_bytes": int(nbytes.value)}
+
+    def close(self):
+        if self.handle:
+            lib().rt_plan_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Engine:
     """One context on one CUDA device."""
 
@@ -356,6 +400,42 @@ class Engine:
         hp = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
         self._check(lib().rt_trace_host(self.ctx, scene.handle, mode, KERNELS[kernel], rp, hp, n))
         return out
+
+    def _batch_array(self, scene: Scene, batches):
+        """(rays, mode[, hits]) tuples -> (ctypes RtBatch array, hit tensors)."""
+        import torch
+        arr = (RtBatch * max(1, len(batches)))()
+        outs = []
+        for i, b in enumerate(batches):
+            rays, mode = b[0], b[1]
+            assert rays.is_cuda and rays.dtype == torch.float32 and rays.is_contiguous()
+            hits = b[2] if len(b) > 2 and b[2] is not None else None
+            words = hit_words(scene.layout, mode)
+            n = rays.shape[0]
+            if hits is None:
+                hits = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=rays.device)
+            arr[i] = RtBatch(rays.data_ptr() if n else None, hits.data_ptr() if n else None, n, mode)
+            outs.append(hits)
+        return arr, outs
+
+    def trace_batches(self, scene: Scene, batches, kernel: str = "fast", stream=None):
+        """Trace many (rays, mode[, hits]) batches of one scene in one persistent launch; returns the
+        hit tensors, one per batch."""
+        import torch
+        arr, outs = self._batch_array(scene, batches)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self._check(lib().rt_trace_batches(self.ctx, scene.handle, KERNELS[kernel], arr, len(batches), s))
+        return outs
+
+    def plan(self, scene: Scene, batches, kernel: str = "fast", refill: int = 0, order: str = "none",
+             graph: bool = True) -> "Plan":
+        """A prepared many-batch launch over fixed buffers (see rt_plan_create)."""
+        arr, outs = self._batch_array(scene, batches)
+        desc = RtPlanDesc(KERNELS[kernel], refill, ORDERS[order], 1 if graph else 0)
+        h = _vp()
+        self._check(lib().rt_plan_create(self.ctx, scene.handle, arr, len(batches), ctypes.byref(desc), ctypes.byref(h)))
+        return Plan(self, scene, h, outs, [b[0] for b in batches], dict(kernel=kernel, refill=refill, order=order,
+                                                                          graph=graph))
 
     def order(self, scene: Scene, rays, key: str = "octant", out=None, stream=None):
         """A permutation of `rays` (CUDA tensor) grouping alike rays; int32 CUDA tensor."""

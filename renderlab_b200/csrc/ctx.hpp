@@ -1,0 +1,102 @@
+// Internal state behind the C ABI's opaque handles, shared by the translation units that
+// implement it (rt_api.cu, batches.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <atomic>
+#include <cstdarg>
+#include <cstdio>
+#include <mutex>
+#include <string>
+
+#include "../../include/rt_trace.h"
+#include "host/host.hpp"
+#include "launch.hpp"
+
+struct rt_scene {
+  uint32_t layout = 0;
+  uint32_t* d_words = nullptr;
+  size_t n_words = 0;
+  rtb::SceneInfo info;
+  size_t device_bytes = 0;
+  void* d_wide8 = nullptr;
+  size_t wide8_bytes = 0;
+  size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
+};
+
+struct rt_blas {
+  rtb::Blas b;
+};
+
+struct rt_ctx {
+  int device = 0;
+  rtk::DevStatus* d_status = nullptr;
+  uint32_t* d_scratch = nullptr;  // 16 words for the self-test
+  // Ray counters of persistent launches: launch k uses slot k mod COUNTER_SLOTS, so up to that
+  // many launches may be in flight at once across streams.
+  unsigned int* d_counters = nullptr;
+  std::atomic<uint64_t> counter_seq{0};
+  rt_tuning tuning = {8, 8, {0, 0, 0, 0, 0, 0}};
+  std::mutex mu;
+  std::string last_error;
+  std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
+  // rt_trace_host staging: two chunks in flight on two streams.
+  cudaStream_t streams[2] = {nullptr, nullptr};
+  void* d_rays = nullptr;
+  void* d_hits = nullptr;
+  size_t stage_rays = 0;  // rays per chunk buffer
+  // rt_order_rays scratch
+  void* d_order_scratch = nullptr;
+  size_t order_scratch_bytes = 0;
+  // rt_trace_batches: batch tables staged through a ring of pinned / device slots, each reused
+  // once the copy that last read it has completed.
+  static constexpr uint32_t TABLE_SLOTS = 8;
+  rtk::BatchEntry* h_tables = nullptr;
+  rtk::BatchEntry* d_tables = nullptr;
+  cudaEvent_t table_done[TABLE_SLOTS] = {};
+  uint32_t table_seq = 0;
+};
+
+namespace rtc {
+
+constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BYTES = 32;
+constexpr uint32_t HOST_CHUNK = 1u << 20;
+constexpr uint32_t COUNTER_SLOTS = 4096;
+
+inline rt_status fail(rt_ctx* ctx, rt_status s, const char* fmt, ...) {
+  if (ctx) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    ctx->last_error = buf;
+  }
+  return s;
+}
+
+#define RT_CUDA(ctx, call)                                                                     \
+  do {                                                                                         \
+    cudaError_t e_ = (call);                                                                   \
+    if (e_ != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+inline size_t hit_bytes(uint32_t layout, uint32_t mode) {
+  if (mode != 0) return ANY_HIT_BYTES;
+  return layout == 0 ? GI_HIT_BYTES : RS_HIT_BYTES;
+}
+
+inline rtl::SceneView view_of(const rt_scene* s) {
+  rtl::SceneView v;
+  v.layout = s->layout;
+  v.words = s->d_words;
+  v.n_words = s->n_words;
+  v.instances = s->info.instances;
+  v.top = s->info.top;
+  v.wide8 = s->d_wide8;
+  v.wide8_bytes = s->wide8_bytes;
+  v.w8_nodes_at = s->w8_nodes_at, v.w8_tris_at = s->w8_tris_at, v.w8_inst_at = s->w8_inst_at;
+  return v;
+}
+
+}  // namespace rtc

@@ -69,6 +69,62 @@ RT_DEV Ray load_ray(const float4* __restrict__ rays, uint32_t i) {
   return Ray{{a.x, a.y, a.z}, a.w, {b.x, b.y, b.z}, b.w};
 }
 
+// One ray batch of a many-batch launch, as the device reads it (32 bytes).
+struct BatchEntry {
+  const float4* rays;
+  void* hits;
+  uint32_t first;  // the entry's first ray in the launch
+  uint32_t n;
+  uint32_t mode;   // 0 closest hit, else any hit
+  uint32_t pad;
+};
+
+// Where a persistent launch's rays come from and where their results go.
+// One batch: ray i of the launch is rays[order ? order[i] : i]; every ray has the launch's mode.
+struct OneBatch {
+  const float4* rays;
+  const uint32_t* order;
+  void* out;
+};
+// Many batches (rt_trace_batches): the launch's ray space is the concatenation of the entries
+// (BatchEntry); a ray's entry is found by binary search over `first`, and each entry has its own
+// rays, results and mode.
+struct ManyBatches {
+  const BatchEntry* table;
+  uint32_t entries;
+  const uint32_t* order;  // optional permutation of the launch's whole ray space
+};
+
+// Mode of a lane: AM 0 closest, 1 any hit, 2 per ray (from its batch entry).
+template <int AM, class Lane>
+RT_DEV bool any_of(const Lane& L) {
+  return AM == 2 ? L.any : AM == 1;
+}
+
+template <class Lane>
+RT_DEV Ray fetch(const OneBatch& s, uint32_t id, Lane& L) {
+  L.ray_id = s.order ? __ldg(s.order + id) : id;
+  L.entry = 0;
+  return load_ray(s.rays, L.ray_id);
+}
+template <class Lane>
+RT_DEV Ray fetch(const ManyBatches& s, uint32_t id, Lane& L) {
+  const uint32_t g = s.order ? __ldg(s.order + id) : id;
+  uint32_t lo = 0, hi = s.entries;  // the last entry whose first ray is at or before g
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (s.table[mid].first <= g) lo = mid;
+    else hi = mid;
+  }
+  const BatchEntry& e = s.table[lo];
+  L.entry = lo;
+  L.ray_id = g - e.first;
+  L.any = e.mode != 0;
+  return load_ray(e.rays, L.ray_id);
+}
+RT_DEV void* out_of(const OneBatch& s, uint32_t) { return s.out; }
+RT_DEV void* out_of(const ManyBatches& s, uint32_t entry) { return s.table[entry].hits; }
+
 // Device-side counters every traversal kernel may bump (rare events only).
 struct DevStatus {
   unsigned long long stack_drops;

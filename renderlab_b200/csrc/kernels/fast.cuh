@@ -47,12 +47,14 @@ RT_DEV uint32_t take_ray(const RayQueue& q, bool need, bool& drained) {
 
 enum : uint32_t { PH_IDLE = 0, PH_TOP = 1, PH_BLAS = 2 };
 
-template <bool ANY>
+template <int AM>
 struct RsLane {
   Ray ray;
   F3 world_inv;
   RsBest best;
   uint32_t ray_id;
+  uint32_t entry;  // batch entry (many-batch launches)
+  bool any;        // any-hit ray (AM 2)
   uint32_t phase;
   // top level (or flat list position)
   uint32_t tsp;
@@ -65,9 +67,9 @@ struct RsLane {
   uint32_t sp;
 };
 
-template <bool ANY>
-RT_DEV void rs_finish(RsLane<ANY>& L, void* __restrict__ out) {
-  if (ANY) {
+template <int AM>
+RT_DEV void rs_finish(RsLane<AM>& L, void* __restrict__ out) {
+  if (any_of<AM>(L)) {
     reinterpret_cast<uint32_t*>(out)[L.ray_id] = L.best.rec[0] != 0 ? 1u : 0u;
   } else {
     uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * (size_t)L.ray_id;
@@ -79,11 +81,11 @@ RT_DEV void rs_finish(RsLane<ANY>& L, void* __restrict__ out) {
 
 // rs_instance's entry (reflections_software_bvh4.wgsl:50-67): true when the lane now walks the
 // instance's BLAS.
-template <bool ANY>
-RT_DEV bool rs_enter(const uint32_t* __restrict__ w, RsLane<ANY>& L, uint32_t i) {
+template <int AM>
+RT_DEV bool rs_enter(const uint32_t* __restrict__ w, RsLane<AM>& L, uint32_t i) {
   const size_t R = 8 + (size_t)i * 24;
   const uint4 tail = ld4(w, R + 20);
-  if (ANY && tail.z != 0) return false;
+  if (any_of<AM>(L) && tail.z != 0) return false;
   const uint4 b0 = ld4(w, R + 12), b1 = ld4(w, R + 16);
   const float bound = rs_limit(L.best, i);
   const F3 lo = {__uint_as_float(b0.x), __uint_as_float(b0.y), __uint_as_float(b0.z)};
@@ -109,8 +111,8 @@ RT_DEV bool rs_enter(const uint32_t* __restrict__ w, RsLane<ANY>& L, uint32_t i)
 }
 
 // One leaf (reflections_software_bvh4.wgsl:72-95). True when an any-hit ray is blocked.
-template <bool ANY>
-RT_DEV bool rs_leaf(const uint32_t* __restrict__ w, RsLane<ANY>& L, uint32_t child) {
+template <int AM>
+RT_DEV bool rs_leaf(const uint32_t* __restrict__ w, RsLane<AM>& L, uint32_t child) {
   const uint32_t start = (child & ~LEAF) >> 4, count = child & 15u;
   const F3 o = L.o, d = L.d;
   for (uint32_t k = 0; k < count; ++k) {
@@ -137,15 +139,15 @@ RT_DEV bool rs_leaf(const uint32_t* __restrict__ w, RsLane<ANY>& L, uint32_t chi
       L.best.rec[0] = L.slot + 1, L.best.rec[1] = w2.y, L.best.rec[2] = __float_as_uint(u);
       L.best.rec[3] = __float_as_uint(v);
       L.best.inst = L.inst;
-      if (ANY) return true;
+      if (any_of<AM>(L)) return true;
     }
   }
   return false;
 }
 
 // One BLAS node (reflections_software_bvh4.wgsl:99-125): children sorted, the nearest kept.
-template <bool ANY>
-RT_DEV void rs_node(const uint32_t* __restrict__ w, RsLane<ANY>& L, uint32_t child, uint32_t* stack, DevStatus* st) {
+template <int AM>
+RT_DEV void rs_node(const uint32_t* __restrict__ w, RsLane<AM>& L, uint32_t child, uint32_t* stack, DevStatus* st) {
   const size_t N = L.nodes + (size_t)child * 16;
   const uint4 n0 = ld4(w, N), n1 = ld4(w, N + 4), n2 = ld4(w, N + 8), n3 = ld4(w, N + 12);
   const float lim = rs_limit(L.best, L.inst);
@@ -181,13 +183,12 @@ RT_DEV void rs_node(const uint32_t* __restrict__ w, RsLane<ANY>& L, uint32_t chi
   L.cur = (dist[0] <= lim && ids[0] != EMPTY) ? ids[0] : EMPTY;
 }
 
-template <bool ANY, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ w, const float4* __restrict__ rays,
-                                                   const uint32_t* __restrict__ order, void* __restrict__ out,
-                                                   RayQueue queue, DevStatus* st) {
+template <int AM, int BLOCK, class Src>
+__global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ w, const Src src, RayQueue queue,
+                                                   DevStatus* st) {
   uint32_t stack[STACK];
   uint32_t top_stack[STACK];
-  RsLane<ANY> L;
+  RsLane<AM> L;
   L.phase = PH_IDLE;
   const uint4 head = ld4(w, 0);
   const size_t bounds = ld(w, 4) & ~3u;
@@ -197,8 +198,7 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
     __syncwarp();
     const uint32_t id = take_ray(queue, L.phase == PH_IDLE, drained);
     if (L.phase == PH_IDLE && id != EMPTY) {
-      L.ray_id = order ? __ldg(order + id) : id;
-      L.ray = load_ray(rays, L.ray_id);
+      L.ray = fetch(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       L.best.t = L.ray.tmax, L.best.rec[0] = L.best.rec[1] = L.best.rec[2] = L.best.rec[3] = 0, L.best.inst = EMPTY;
       // rs_trace prologue (reflections_software_bvh4.wgsl:141-155)
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
         L.tsp = 1;
         top_stack[0] = head.z;
       } else {
-        rs_finish<ANY>(L, out);  // misses the scene box: done, refilled next iteration
+        rs_finish<AM>(L, out_of(src, L.entry));  // misses the scene box: done, refilled next iteration
       }
     }
     // Every lane reaches this vote once per iteration (no exit above it); the warp leaves only
@@ -239,13 +239,13 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
       if (L.phase == PH_BLAS) {
         const uint32_t child = L.cur;
         if (child & LEAF) {
-          if (rs_leaf<ANY>(w, L, child)) {
-            rs_finish<ANY>(L, out);
+          if (rs_leaf<AM>(w, L, child)) {
+            rs_finish<AM>(L, out_of(src, L.entry));
             continue;
           }
           L.cur = EMPTY;
         } else {
-          rs_node<ANY>(w, L, child, stack, st);
+          rs_node<AM>(w, L, child, stack, st);
         }
         continue;
       }
@@ -253,19 +253,19 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
     if (L.phase == PH_TOP) {
       if (head.y == 0) {  // flat instance list
         if (L.flat_i >= head.x) {
-          rs_finish<ANY>(L, out);
+          rs_finish<AM>(L, out_of(src, L.entry));
           continue;
         }
-        rs_enter<ANY>(w, L, L.flat_i++);
+        rs_enter<AM>(w, L, L.flat_i++);
         continue;
       }
       if (L.tsp == 0) {
-        rs_finish<ANY>(L, out);
+        rs_finish<AM>(L, out_of(src, L.entry));
         continue;
       }
       const uint32_t item = top_stack[--L.tsp];
       if (item & LEAF) {
-        rs_enter<ANY>(w, L, item & ~LEAF);
+        rs_enter<AM>(w, L, item & ~LEAF);
         continue;
       }
       const float bound = L.best.rec[0] != 0 ? next_up(L.best.t) : L.best.t;
@@ -276,12 +276,14 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
 
 // ---------------------------------------------------------------- GI layout
 
-template <bool ANY>
+template <int AM>
 struct GiLane {
   Ray ray;
   F3 world_inv;
   GiBest best;
   uint32_t ray_id;
+  uint32_t entry;
+  bool any;
   uint32_t phase;
   uint32_t tsp, flat_i;
   uint32_t inst;
@@ -291,10 +293,10 @@ struct GiLane {
   uint32_t cur, sp;
 };
 
-template <bool ANY>
-RT_DEV void gi_finish(GiLane<ANY>& L, void* __restrict__ out) {
+template <int AM>
+RT_DEV void gi_finish(GiLane<AM>& L, void* __restrict__ out) {
   const GiBest& b = L.best;
-  if (ANY) {
+  if (any_of<AM>(L)) {
     reinterpret_cast<uint32_t*>(out)[L.ray_id] = b.hit ? 1u : 0u;
   } else {
     uint32_t* o = reinterpret_cast<uint32_t*>(out) + 10 * (size_t)L.ray_id;
@@ -306,10 +308,10 @@ RT_DEV void gi_finish(GiLane<ANY>& L, void* __restrict__ out) {
 }
 
 // gi_instance's entry (gi_rays_software.wgsl:100-113)
-template <bool ANY>
-RT_DEV void gi_enter(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t i) {
+template <int AM>
+RT_DEV void gi_enter(const uint32_t* __restrict__ w, GiLane<AM>& L, uint32_t i) {
   const size_t r = 16 + (size_t)i * 32;
-  if (ANY && (ld(w, r + 27) & 1u) != 0) return;
+  if (any_of<AM>(L) && (ld(w, r + 27) & 1u) != 0) return;
   const float lim = gi_limit(L.best, i);
   if (!(slab_near(L.ray.o, L.world_inv, ld3(w, r + 12), ld3(w, r + 15), L.ray.tmin, lim) <= lim)) return;
   for (int k = 0; k < 12; ++k) L.r[k] = ldf(w, r + k);
@@ -327,8 +329,8 @@ RT_DEV void gi_enter(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t i)
 }
 
 // One GI leaf (gi_rays_software.wgsl:117-169). True when an any-hit ray is blocked.
-template <bool ANY>
-RT_DEV bool gi_leaf(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t child) {
+template <int AM>
+RT_DEV bool gi_leaf(const uint32_t* __restrict__ w, GiLane<AM>& L, uint32_t child) {
   const size_t l = L.leaves + (size_t)(child & ~LEAF) * 2;
   const uint32_t first = ld(w, l), count = ld(w, l + 1);
   const uint32_t i = L.inst;
@@ -352,14 +354,14 @@ RT_DEV bool gi_leaf(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t chi
     float t, u, v;
     if (gi_triangle(L.o, L.d, a, b, c, L.ray.tmin, gi_limit(L.best, i), t, u, v)) {
       L.best.hit = true, L.best.t = t, L.best.inst = i, L.best.u = u, L.best.v = v;
-      if (ANY) return true;
+      if (any_of<AM>(L)) return true;
       L.best.n = normal_of(a, b, c);
       if (L.prim_base != 0) L.best.tri[0] = ld(w, L.prim_base + (first + k) / 3), L.best.tri[1] = 0, L.best.tri[2] = 0;
       else L.best.tri[0] = ia, L.best.tri[1] = ib, L.best.tri[2] = ic;
     }
     if (two && gi_triangle(L.o, L.d, a2, b2, c2, L.ray.tmin, gi_limit(L.best, i), t, u, v)) {
       L.best.hit = true, L.best.t = t, L.best.inst = i, L.best.u = u, L.best.v = v;
-      if (ANY) return true;
+      if (any_of<AM>(L)) return true;
       L.best.n = normal_of(a2, b2, c2);
       if (L.prim_base != 0) L.best.tri[0] = ld(w, L.prim_base + (first + k) / 3 + 1), L.best.tri[1] = 0, L.best.tri[2] = 0;
       else L.best.tri[0] = ja, L.best.tri[1] = jb, L.best.tri[2] = jc;
@@ -369,8 +371,8 @@ RT_DEV bool gi_leaf(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t chi
 }
 
 // One GI BLAS node (gi_rays_software.wgsl:171-204): every surviving child pushed far to near.
-template <bool ANY>
-RT_DEV void gi_node(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t child, uint32_t* stack, DevStatus* st) {
+template <int AM>
+RT_DEV void gi_node(const uint32_t* __restrict__ w, GiLane<AM>& L, uint32_t child, uint32_t* stack, DevStatus* st) {
   const size_t n = L.nodes + (size_t)child * 16;
   const uint4 n0 = ld4(w, n), n1 = ld4(w, n + 4), n2 = ld4(w, n + 8), n3 = ld4(w, n + 12);
   const F3 oq = {__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z)};
@@ -406,13 +408,12 @@ RT_DEV void gi_node(const uint32_t* __restrict__ w, GiLane<ANY>& L, uint32_t chi
   L.cur = EMPTY;
 }
 
-template <bool ANY, int BLOCK>
-__global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ w, const float4* __restrict__ rays,
-                                                   const uint32_t* __restrict__ order, void* __restrict__ out,
-                                                   RayQueue queue, DevStatus* st) {
+template <int AM, int BLOCK, class Src>
+__global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ w, const Src src, RayQueue queue,
+                                                   DevStatus* st) {
   uint32_t stack[STACK];
   uint32_t top_stack[STACK];
-  GiLane<ANY> L;
+  GiLane<AM> L;
   L.phase = PH_IDLE;
   const uint32_t instances = ld(w, 0), top = ld(w, 1), root = ld(w, 2);
   bool drained = false;
@@ -420,8 +421,7 @@ __global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ 
     __syncwarp();
     const uint32_t id = take_ray(queue, L.phase == PH_IDLE, drained);
     if (L.phase == PH_IDLE && id != EMPTY) {
-      L.ray_id = order ? __ldg(order + id) : id;
-      L.ray = load_ray(rays, L.ray_id);
+      L.ray = fetch(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       L.best.hit = false, L.best.t = L.ray.tmax, L.best.n = {0.0f, 0.0f, 0.0f}, L.best.inst = EMPTY;
       L.best.tri[0] = L.best.tri[1] = L.best.tri[2] = 0, L.best.u = L.best.v = 0.0f;
@@ -442,13 +442,13 @@ __global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ 
       if (L.phase == PH_BLAS) {
         const uint32_t child = L.cur;
         if (child & LEAF) {
-          if (gi_leaf<ANY>(w, L, child)) {
-            gi_finish<ANY>(L, out);
+          if (gi_leaf<AM>(w, L, child)) {
+            gi_finish<AM>(L, out_of(src, L.entry));
             continue;
           }
           L.cur = EMPTY;
         } else {
-          gi_node<ANY>(w, L, child, stack, st);
+          gi_node<AM>(w, L, child, stack, st);
         }
         continue;
       }
@@ -456,19 +456,19 @@ __global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ 
     if (L.phase == PH_TOP) {
       if (top == 0) {
         if (L.flat_i >= instances) {
-          gi_finish<ANY>(L, out);
+          gi_finish<AM>(L, out_of(src, L.entry));
           continue;
         }
-        gi_enter<ANY>(w, L, L.flat_i++);
+        gi_enter<AM>(w, L, L.flat_i++);
         continue;
       }
       if (L.tsp == 0) {
-        gi_finish<ANY>(L, out);
+        gi_finish<AM>(L, out_of(src, L.entry));
         continue;
       }
       const uint32_t item = top_stack[--L.tsp];
       if (item & LEAF) {
-        gi_enter<ANY>(w, L, item & ~LEAF);
+        gi_enter<AM>(w, L, item & ~LEAF);
         continue;
       }
       const float bound = L.best.hit ? next_up(L.best.t) : L.best.t;

@@ -198,9 +198,9 @@ RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, 
 }
 
 // Considers one candidate triangle; returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, bool ANY, bool COUNT>
+template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const W8Ray& R, const Ray& ray, uint32_t inst,
-                         uint32_t tri, W8Best& best, unsigned long long* cnt) {
+                         uint32_t tri, W8Best& best, unsigned long long* cnt, bool lane_any) {
   w8_count<COUNT>(cnt, W8C_TRIS);
   const uint4 q0 = __ldg(V.tris + 3 * (size_t)tri), q1 = __ldg(V.tris + 3 * (size_t)tri + 1),
               q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
@@ -250,7 +250,7 @@ RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const 
     best.abs_err = abs_err;
   }
   best.inst = inst, best.tri = tri, best.ident = ident;
-  return ANY;
+  return AM == 2 ? lane_any : AM == 1;
 }
 
 // XOR-permute an 8-bit slot mask: bit k of the result is bit (k ^ o) of m.
@@ -270,7 +270,8 @@ struct W8Lane {
   Ray ray;
   F3 world_inv;
   W8Best best;
-  uint32_t ray_id, phase;
+  uint32_t ray_id, entry, phase;
+  bool any;
   uint32_t tsp, flat;
   uint32_t inst;
   W8Ray R;
@@ -281,7 +282,7 @@ struct W8Lane {
 
 // One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
 // Returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, bool ANY, bool COUNT>
+template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st,
                     unsigned long long* cnt) {
   w8_count<COUNT>(cnt, W8C_NODES);
@@ -339,7 +340,7 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
     const uint32_t first = tri_base + (m & 31u), count = m >> 5;
     w8_count<COUNT>(cnt, W8C_LEAVES);
     for (uint32_t k = 0; k < count; ++k)
-      if (w8_candidate<LAYOUT, ANY, COUNT>(w, V, R, L.ray, L.inst, first + k, L.best, cnt)) return true;
+      if (w8_candidate<LAYOUT, AM, COUNT>(w, V, R, L.ray, L.inst, first + k, L.best, cnt, L.any)) return true;
   }
   const uint32_t inner = oct_permute(hits & imask, R.oct);
   if (inner) {
@@ -368,10 +369,10 @@ RT_DEV bool w8_next(W8Lane& L, const uint2* stack) {
 }
 
 // Enters instance i when its world box survives; sets up the object-space ray.
-template <uint32_t LAYOUT, bool ANY, bool COUNT>
+template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i, unsigned long long* cnt) {
   const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;
-  if (ANY && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
+  if (any_of<AM>(L) && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
   const W8Best& best = L.best;
   const float bound = best.hit ? best.t + 2.0f * best.band + 2.0f * W8_TIE * best.t : L.ray.tmax;
   if (!(slab_near(L.ray.o, L.world_inv, ld3(w, r + 12), ld3(w, r + 15), L.ray.tmin, bound) <= bound)) return;
@@ -391,14 +392,14 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   L.phase = 2;
 }
 
-template <uint32_t LAYOUT, bool ANY, bool COUNT>
+template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, void* __restrict__ out,
                       unsigned long long* cnt) {
   w8_count<COUNT>(cnt, W8C_RAYS);
   W8Best& b = L.best;
   const uint32_t id = L.ray_id;
   L.phase = 0;
-  if (ANY) {
+  if (any_of<AM>(L)) {
     reinterpret_cast<uint32_t*>(out)[id] = b.hit ? 1u : 0u;
     return;
   }
@@ -445,9 +446,8 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
 // Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
 // step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
 // re-converges at the top of the loop.
-template <uint32_t LAYOUT, bool ANY, int BLOCK, bool COUNT>
-__global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__ w, W8View V, const float4* __restrict__ rays,
-                                                 const uint32_t* __restrict__ order, void* __restrict__ out,
+template <uint32_t LAYOUT, int AM, int BLOCK, bool COUNT, class Src>
+__global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                  unsigned int* __restrict__ counter, uint32_t n, DevStatus* st,
                                                  unsigned long long* cnt, uint32_t refill) {
   uint2 stack[W8_STACK];
@@ -474,8 +474,7 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__
       if ((want >> lane & 1u) && idx < n) id = idx;
     }
     if (id != EMPTY) {
-      L.ray_id = order ? __ldg(order + id) : id;
-      L.ray = load_ray(rays, L.ray_id);
+      L.ray = fetch(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
       b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.abs_err = 0.0f, b.t64 = 0.0;
@@ -493,26 +492,26 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__
       if (L.node == EMPTY && !w8_next(L, stack)) {
         L.phase = 1;
       } else {
-        if (w8_node<LAYOUT, ANY, COUNT>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, ANY, COUNT>(w, V, L, out, cnt);
+        if (w8_node<LAYOUT, AM, COUNT>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, AM, COUNT>(w, V, L, out_of(src, L.entry), cnt);
         continue;
       }
     }
     if (L.phase == 1) {
       if (top == 0) {
         if (L.flat >= count) {
-          w8_finish<LAYOUT, ANY, COUNT>(w, V, L, out, cnt);
+          w8_finish<LAYOUT, AM, COUNT>(w, V, L, out_of(src, L.entry), cnt);
           continue;
         }
-        w8_enter<LAYOUT, ANY, COUNT>(w, V, L, L.flat++, cnt);
+        w8_enter<LAYOUT, AM, COUNT>(w, V, L, L.flat++, cnt);
         continue;
       }
       if (L.tsp == 0) {
-        w8_finish<LAYOUT, ANY, COUNT>(w, V, L, out, cnt);
+        w8_finish<LAYOUT, AM, COUNT>(w, V, L, out_of(src, L.entry), cnt);
         continue;
       }
       const uint32_t item = tstack[--L.tsp];
       if (item & LEAF) {
-        w8_enter<LAYOUT, ANY, COUNT>(w, V, L, item & ~LEAF, cnt);
+        w8_enter<LAYOUT, AM, COUNT>(w, V, L, item & ~LEAF, cnt);
         continue;
       }
       const W8Best& b = L.best;

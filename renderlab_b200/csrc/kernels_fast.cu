@@ -36,14 +36,14 @@ cudaError_t grid_for(K kernel, uint32_t n, dim3& grid) {
   return cudaSuccess;
 }
 
-template <class K>
-cudaError_t run(K kernel, const SceneView& s, const float4* rays, const uint32_t* order, void* hits, uint32_t n,
-                unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
+template <class K, class Src>
+cudaError_t run(K kernel, const SceneView& s, const Src& src, uint32_t n, unsigned int* counter, rtk::DevStatus* st,
+                cudaStream_t stream, uint32_t refill) {
   dim3 grid;
   cudaError_t e = grid_for(kernel, n, grid);
   if (e != cudaSuccess) return e;
   if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-  kernel<<<grid, FAST_BLOCK, 0, stream>>>(s.words, rays, order, hits, rtk::RayQueue{counter, n, refill}, st);
+  kernel<<<grid, FAST_BLOCK, 0, stream>>>(s.words, src, rtk::RayQueue{counter, n, refill}, st);
   return cudaGetLastError();
 }
 }  // namespace
@@ -51,12 +51,24 @@ cudaError_t run(K kernel, const SceneView& s, const float4* rays, const uint32_t
 cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
   if (n == 0) return cudaSuccess;
+  using rtk::OneBatch;
+  const OneBatch src{rays, order, hits};
   if (s.layout == 0) {
-    if (mode == 0) return run(rtk::k_gi_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
-    return run(rtk::k_gi_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
+    if (mode == 0) return run(rtk::k_gi_fast<0, FAST_BLOCK, OneBatch>, s, src, n, counter, st, stream, refill);
+    return run(rtk::k_gi_fast<1, FAST_BLOCK, OneBatch>, s, src, n, counter, st, stream, refill);
   }
-  if (mode == 0) return run(rtk::k_rs_fast<false, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
-  return run(rtk::k_rs_fast<true, FAST_BLOCK>, s, rays, order, hits, n, counter, st, stream, refill);
+  if (mode == 0) return run(rtk::k_rs_fast<0, FAST_BLOCK, OneBatch>, s, src, n, counter, st, stream, refill);
+  return run(rtk::k_rs_fast<1, FAST_BLOCK, OneBatch>, s, src, n, counter, st, stream, refill);
+}
+
+cudaError_t launch_fast_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
+                                const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
+                                uint32_t refill) {
+  if (total == 0) return cudaSuccess;
+  using rtk::ManyBatches;
+  const ManyBatches src{table, entries, order};
+  if (s.layout == 0) return run(rtk::k_gi_fast<2, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+  return run(rtk::k_rs_fast<2, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
 }
 
 }  // namespace rtl

@@ -25,11 +25,19 @@ __device__ __forceinline__ uint32_t cell(float v, float lo, float scale, uint32_
 
 // kind 1: 30-bit Morton code of the origin; kind 2: direction octant (3 bits) above a 27-bit
 // Morton code of the origin; kind 3: a 12-bit octahedral direction cell above an 18-bit origin code.
-__global__ void k_keys(const float4* __restrict__ rays, uint32_t n, float3 lo, float3 inv_ext, uint32_t kind,
-                       uint32_t* __restrict__ keys, uint32_t* __restrict__ vals) {
+struct KeyLane {
+  uint32_t ray_id, entry;
+  bool any;
+};
+
+template <class Src>
+__global__ void k_keys(const Src src, uint32_t n, float3 lo, float3 inv_ext, uint32_t kind, uint32_t* __restrict__ keys,
+                       uint32_t* __restrict__ vals) {
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
+  KeyLane lane;
+  const rtk::Ray r = rtk::fetch(src, i, lane);
+  const float3 a = make_float3(r.o.x, r.o.y, r.o.z), b = make_float3(r.d.x, r.d.y, r.d.z);
   uint32_t key;
   if (kind == 1) {
     key = spread3(cell(a.x, lo.x, 1024.0f * inv_ext.x, 1023)) | spread3(cell(a.y, lo.y, 1024.0f * inv_ext.y, 1023)) << 1 |
@@ -64,8 +72,10 @@ size_t order_scratch_bytes(uint32_t n) {
   return 3 * (size_t)n * sizeof(uint32_t) + ((temp + 255) & ~(size_t)255) + 256;
 }
 
-cudaError_t launch_order(const float4* rays, uint32_t n, const float lo[3], const float hi[3], uint32_t kind,
-                         uint32_t* order, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+namespace {
+template <class Src>
+cudaError_t order_any(const Src& src, uint32_t n, const float lo[3], const float hi[3], uint32_t kind, uint32_t* order,
+                      void* scratch, size_t scratch_bytes, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   if (scratch_bytes < order_scratch_bytes(n)) return cudaErrorInvalidValue;
   uint32_t* keys_in = static_cast<uint32_t*>(scratch);
@@ -74,12 +84,24 @@ cudaError_t launch_order(const float4* rays, uint32_t n, const float lo[3], cons
   void* temp = reinterpret_cast<void*>((reinterpret_cast<uintptr_t>(vals_in + n) + 255) & ~(uintptr_t)255);
   size_t temp_bytes = scratch_bytes - (static_cast<char*>(temp) - static_cast<char*>(scratch));
   auto inv = [](float a, float b) { return b > a ? 1.0f / (b - a) : 1.0f; };
-  k_keys<<<(n + 255) / 256, 256, 0, stream>>>(rays, n, make_float3(lo[0], lo[1], lo[2]),
+  k_keys<<<(n + 255) / 256, 256, 0, stream>>>(src, n, make_float3(lo[0], lo[1], lo[2]),
                                               make_float3(inv(lo[0], hi[0]), inv(lo[1], hi[1]), inv(lo[2], hi[2])), kind,
                                               keys_in, vals_in);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) return e;
   return cub::DeviceRadixSort::SortPairs(temp, temp_bytes, keys_in, keys_out, vals_in, order, (int)n, 0, 32, stream);
+}
+}  // namespace
+
+cudaError_t launch_order(const float4* rays, uint32_t n, const float lo[3], const float hi[3], uint32_t kind,
+                         uint32_t* order, void* scratch, size_t scratch_bytes, cudaStream_t stream) {
+  return order_any(rtk::OneBatch{rays, nullptr, nullptr}, n, lo, hi, kind, order, scratch, scratch_bytes, stream);
+}
+
+cudaError_t launch_order_batches(const rtk::BatchEntry* table, uint32_t entries, uint32_t total, const float lo[3],
+                                 const float hi[3], uint32_t kind, uint32_t* order, void* scratch, size_t scratch_bytes,
+                                 cudaStream_t stream) {
+  return order_any(rtk::ManyBatches{table, entries, nullptr}, total, lo, hi, kind, order, scratch, scratch_bytes, stream);
 }
 
 }  // namespace rtl

@@ -23,17 +23,25 @@ cudaError_t resident(K kernel, uint32_t& out) {
   return cudaSuccess;
 }
 
-template <class K>
-cudaError_t run(K kernel, const uint32_t* words, const rtk::W8View& v, const float4* rays, const uint32_t* order,
-                void* hits, unsigned int* counter, uint32_t n, rtk::DevStatus* st, cudaStream_t stream,
-                unsigned long long* cnt, uint32_t refill) {
+template <class K, class Src>
+cudaError_t run(K kernel, const uint32_t* words, const rtk::W8View& v, const Src& src, unsigned int* counter, uint32_t n,
+                rtk::DevStatus* st, cudaStream_t stream, unsigned long long* cnt, uint32_t refill) {
   uint32_t full = 0;
   cudaError_t e = resident(kernel, full);
   if (e != cudaSuccess) return e;
   const uint32_t need = (n + W8_BLOCK - 1) / W8_BLOCK;
   if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
-  kernel<<<need < full ? need : full, W8_BLOCK, 0, stream>>>(words, v, rays, order, hits, counter, n, st, cnt, refill);
+  kernel<<<need < full ? need : full, W8_BLOCK, 0, stream>>>(words, v, src, counter, n, st, cnt, refill);
   return cudaGetLastError();
+}
+
+bool view_of(const SceneView& s, rtk::W8View& v) {
+  if (!s.wide8) return false;
+  const uint32_t* base = static_cast<const uint32_t*>(s.wide8);
+  v.nodes = reinterpret_cast<const uint4*>(base + s.w8_nodes_at);
+  v.tris = reinterpret_cast<const uint4*>(base + s.w8_tris_at);
+  v.inst = base + s.w8_inst_at;
+  return true;
 }
 
 template <bool COUNT>
@@ -41,18 +49,16 @@ cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, co
                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
                        unsigned long long* cnt, uint32_t refill) {
   if (n == 0) return cudaSuccess;
-  if (!s.wide8) return cudaErrorInvalidValue;
   rtk::W8View v;
-  const uint32_t* base = static_cast<const uint32_t*>(s.wide8);
-  v.nodes = reinterpret_cast<const uint4*>(base + s.w8_nodes_at);
-  v.tris = reinterpret_cast<const uint4*>(base + s.w8_tris_at);
-  v.inst = base + s.w8_inst_at;
+  if (!view_of(s, v)) return cudaErrorInvalidValue;
+  using rtk::OneBatch;
+  const OneBatch src{rays, order, hits};
   if (s.layout == 0) {
-    if (mode == 0) return run(rtk::k_wide8<0, false, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
-    return run(rtk::k_wide8<0, true, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
+    if (mode == 0) return run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
+    return run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
   }
-  if (mode == 0) return run(rtk::k_wide8<1, false, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
-  return run(rtk::k_wide8<1, true, W8_BLOCK, COUNT>, s.words, v, rays, order, hits, counter, n, st, stream, cnt, refill);
+  if (mode == 0) return run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
+  return run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
 }
 
 cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
@@ -63,6 +69,19 @@ cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, 
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream) {
   return launch_any<true>(s, mode, rays, nullptr, hits, n, counter, st, stream, cnt, 1);
+}
+
+cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
+                                 const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
+                                 uint32_t refill) {
+  if (total == 0) return cudaSuccess;
+  rtk::W8View v;
+  if (!view_of(s, v)) return cudaErrorInvalidValue;
+  using rtk::ManyBatches;
+  const ManyBatches src{table, entries, order};
+  if (s.layout == 0)
+    return run(rtk::k_wide8<0, 2, W8_BLOCK, false, ManyBatches>, s.words, v, src, counter, total, st, stream, nullptr, refill);
+  return run(rtk::k_wide8<1, 2, W8_BLOCK, false, ManyBatches>, s.words, v, src, counter, total, st, stream, nullptr, refill);
 }
 
 }  // namespace rtl

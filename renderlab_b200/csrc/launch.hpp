@@ -32,6 +32,14 @@ cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, c
 // `refill`: idle lanes (1-32) a warp waits for before it takes more rays.
 cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                          uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
+// Many batches in one persistent launch: `table` (device, `entries` records sorted by `first`)
+// covers `total` rays; `order` (optional) permutes the launch's ray space. Mode per entry.
+cudaError_t launch_fast_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
+                                const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
+                                uint32_t refill);
+cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
+                                 const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
+                                 uint32_t refill);
 // WIDE8 with per-event device counters (rtk::W8Count order) accumulated into cnt[8].
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream);
@@ -40,6 +48,10 @@ cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, v
 size_t order_scratch_bytes(uint32_t n);
 cudaError_t launch_order(const float4* rays, uint32_t n, const float lo[3], const float hi[3], uint32_t kind,
                          uint32_t* order, void* scratch, size_t scratch_bytes, cudaStream_t stream);
+// The same over a many-batch launch's ray space (its batch table).
+cudaError_t launch_order_batches(const rtk::BatchEntry* table, uint32_t entries, uint32_t total, const float lo[3],
+                                 const float hi[3], uint32_t kind, uint32_t* order, void* scratch, size_t scratch_bytes,
+                                 cudaStream_t stream);
 cudaError_t launch_selftest(uint32_t* out16, cudaStream_t stream);
 
 }  // namespace rtl

@@ -13,88 +13,14 @@
 #include <vector>
 
 #include "../../include/rt_trace.h"
+#include "ctx.hpp"
 #include "host/host.hpp"
 #include "host/wide8.hpp"
 #include "launch.hpp"
 
-struct rt_scene {
-  uint32_t layout = 0;
-  uint32_t* d_words = nullptr;
-  size_t n_words = 0;
-  rtb::SceneInfo info;
-  size_t device_bytes = 0;
-  void* d_wide8 = nullptr;
-  size_t wide8_bytes = 0;
-  size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
-};
-
-struct rt_blas {
-  rtb::Blas b;
-};
-
-struct rt_ctx {
-  int device = 0;
-  rtk::DevStatus* d_status = nullptr;
-  uint32_t* d_scratch = nullptr;  // 16 words for the self-test
-  // Ray counters of persistent launches: launch k uses slot k mod COUNTER_SLOTS, so up to that
-  // many launches may be in flight at once across streams.
-  unsigned int* d_counters = nullptr;
-  std::atomic<uint64_t> counter_seq{0};
-  rt_tuning tuning = {8, 8, {0, 0, 0, 0, 0, 0}};
-  std::mutex mu;
-  std::string last_error;
-  std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
-  // rt_trace_host staging: two chunks in flight on two streams.
-  cudaStream_t streams[2] = {nullptr, nullptr};
-  void* d_rays = nullptr;
-  void* d_hits = nullptr;
-  size_t stage_rays = 0;  // rays per chunk buffer
-  // rt_order_rays scratch
-  void* d_order_scratch = nullptr;
-  size_t order_scratch_bytes = 0;
-};
+using namespace rtc;
 
 namespace {
-
-constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BYTES = 32;
-constexpr uint32_t HOST_CHUNK = 1u << 20;
-constexpr uint32_t COUNTER_SLOTS = 4096;
-
-rt_status fail(rt_ctx* ctx, rt_status s, const char* fmt, ...) {
-  if (ctx) {
-    char buf[512];
-    va_list ap;
-    va_start(ap, fmt);
-    std::vsnprintf(buf, sizeof buf, fmt, ap);
-    va_end(ap);
-    ctx->last_error = buf;
-  }
-  return s;
-}
-
-#define RT_CUDA(ctx, call)                                                                     \
-  do {                                                                                         \
-    cudaError_t e_ = (call);                                                                   \
-    if (e_ != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
-  } while (0)
-
-size_t hit_bytes(uint32_t layout, uint32_t mode) {
-  if (mode != 0) return ANY_HIT_BYTES;
-  return layout == 0 ? GI_HIT_BYTES : RS_HIT_BYTES;
-}
-
-rtl::SceneView view_of(const rt_scene* s) {
-  rtl::SceneView v;
-  v.layout = s->layout;
-  v.words = s->d_words;
-  v.n_words = s->n_words;
-  v.instances = s->info.instances;
-  v.top = s->info.top;
-  v.wide8 = s->d_wide8;
-  v.wide8_bytes = s->wide8_bytes;
-  v.w8_nodes_at = s->w8_nodes_at, v.w8_tris_at = s->w8_tris_at, v.w8_inst_at = s->w8_inst_at;
-  return v;
-}
 
 rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* rays,
                    const uint32_t* order, void* hits, uint32_t n, cudaStream_t stream) {
@@ -169,6 +95,10 @@ void rt_ctx_destroy(rt_ctx* ctx) {
   cudaFree(ctx->d_rays);
   cudaFree(ctx->d_hits);
   cudaFree(ctx->d_order_scratch);
+  cudaFree(ctx->d_tables);
+  cudaFreeHost(ctx->h_tables);
+  for (cudaEvent_t e : ctx->table_done)
+    if (e) cudaEventDestroy(e);
   delete ctx;
 }
 
