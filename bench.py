@@ -1,12 +1,23 @@
-"""Traversal benchmark: Mrays/s on the 1M-triangle cluster scene, one JSON line on stdout.
+"""Traversal benchmark: Mrays/s of the tuned traversal against the plain kernel at matched hits,
+one JSON line on stdout.
 
-Workload (one step): 4,194,304 coherent primary rays (2048 x 2048 pinhole from (0, 0, -250),
-fov 60 deg) plus 4,194,304 cosine-hemisphere GI rays spawned from the primary hits, closest hit,
-over 1,000,000 triangles in 2,000 seeded clusters, packed in renderlab's reflection layout
-(BVH4 with 8-bit child boxes, 48-byte pre-edged triangles). Inputs are synthetic and seeded
-(splitmix64), the scene is device resident; L2 is flushed (a 256 MiB write) before each step.
+Workloads (seeded synthetic scenes and rays; splitmix64, seed 0x5EED0000 + config):
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--kernel plain|fast|wide8]
+* --config 2 (default) clusters-1M: 1,000,000 triangles in 2,000 clusters, reflection layout;
+  per step 4,194,304 coherent primary rays (2048 x 2048 pinhole from (0, 0, -250), fov 60 deg)
+  plus 4,194,304 cosine-hemisphere GI rays spawned from the primary hits, closest hit.
+* --config 1 cubes-120k: 10,000 jittered unit cubes merged into one BLAS, GI layout; 1024 x 1024
+  primaries closest hit plus one sun any-hit ray per hit.
+* --config 3 precision-4M: 4,000,000 cluster triangles; 16,777,216 mixed rays: 50 % primary
+  (4096 x 2048), 30 % GI hemisphere, 20 % shadow any-hit toward 16 point lights.
+* --config 4 batching: 64 BLAS (2k-500k triangles, log-uniform) under 10,000 randomly rotated,
+  scaled and placed instances; 64 ray batches (1k-2M rays, log-uniform), closest / any hit.
+
+Per step, the "plain" arm launches the plain kernel once per batch; the product arm replays the
+plans the autotuner chose (kernel, wavefront width, sort key; one CUDA graph per plan). Scenes
+and rays are device resident; L2 is flushed (a 256 MiB write) before each step.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--config 1|2|3|4] [--kernel auto|plain|fast|wide8]
     python bench.py --impl reference ...   # the reference CPU traversal on the host cores
 
 Under torchrun (N > 1) every rank traces the full per-GPU workload on its own GPU (rays are
@@ -20,8 +31,8 @@ import os
 import subprocess
 import sys
 import tempfile
-import threading
 import time
+from dataclasses import dataclass, field
 from pathlib import Path
 
 import numpy as np
@@ -31,57 +42,148 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "Mrays/s closest+any-hit vs plain kernel at matched hits, 1 B200; p50/p99 latency"
 UNIT = "Mrays/s"
-WORKLOAD = ("clusters-1M: 1,000,000 triangles in 2,000 clusters (reflection layout); "
-            "4,194,304 primary + 4,194,304 GI hemisphere rays per step, closest hit")
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--kernel", default="auto")
-    ap.add_argument("--triangles", type=int, default=1_000_000)
-    ap.add_argument("--width", type=int, default=2048)
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4])
+    ap.add_argument("--kernel", default="auto", help="auto: the autotuner's choice; or plain / fast / wide8")
+    ap.add_argument("--refill", type=int, default=0, help="with --kernel fast/wide8: the wavefront width")
+    ap.add_argument("--order", default="none", help="with --kernel fast/wide8: the sort key")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--refill", type=int, default=0, help="persistent-kernel refill threshold (lanes)")
-    return ap.parse_args()
+    ap.add_argument("--small", action="store_true", help="a reduced workload (profiling captures)")
+    return ap.parse_args(argv)
 
 
-# ---------------------------------------------------------------- workload
+# ---------------------------------------------------------------- workloads
 
-def make_scene(n_tris):
-    from renderlab_b200 import api as A
-    from renderlab_b200 import scenes as S
-    mesh = S.clusters(n_tris, config=2)
-    words = A.pack_scene(A.LAYOUT_REFLECTION, [A.Blas(mesh.positions, mesh.indices)], S.identity_instances(1))
-    return mesh, words
+@dataclass
+class Batch:
+    label: str
+    rays: np.ndarray  # (n, 8) float32
+    mode: int         # 0 closest, 1/2 any hit
 
 
-def make_rays(engine, scene, mesh, width, kernel):
-    """Primary rays, then one GI ray per primary ray, spawned from the primary hits in turn."""
+@dataclass
+class Workload:
+    name: str
+    layout: int
+    words: np.ndarray
+    batches: list
+    groups: list            # one tuned plan per group of batch indices
+    triangles: int
+    info: dict = field(default_factory=dict)
+
+    @property
+    def rays(self) -> int:
+        return sum(len(b.rays) for b in self.batches)
+
+
+def gpu_closest(engine, scene, rays, mode):
+    """Rays traced by the plain kernel; the hits of a step's first batch spawn its later ones."""
     import torch
+    h = engine.trace(scene, torch.from_numpy(rays).cuda(), mode, "plain")
+    torch.cuda.synchronize()
+    return h.cpu().numpy().view(np.uint32)
+
+
+def _hits(layout, h):
+    """(hit mask, t, primitive column) of closest-hit results."""
+    from renderlab_b200 import api as A
+    if layout == A.LAYOUT_GI:
+        return h[:, 1] != A.MISS, h[:, 0].view(np.float32), h[:, 2]
+    return h[:, 1] != 0, h[:, 0].view(np.float32), h[:, 2]
+
+
+def engine_pack(layout, meshes, instances, primitives=None):
+    """Packed words from the engine's host builders (rt_blas_build, rt_pack_scene)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from renderlab_b200 import api as A
+    with ThreadPoolExecutor(min(16, os.cpu_count() or 1)) as ex:
+        blas = list(ex.map(lambda m: A.Blas(m.positions, m.indices), meshes))
+    return A.pack_scene(layout, blas, instances, primitives=primitives)
+
+
+def oracle_pack(layout, meshes, instances, primitives=None):
+    """Packed words from the oracle's restatement of the reference builders and packers."""
+    from oracle import oracle as O
+    n = len(instances)
+    if layout == 0:
+        aux = np.zeros((n, 9), np.uint32)
+        aux[:, 4] = (~instances.casts).astype(np.uint32)
+    else:
+        aux = np.stack([np.arange(n), instances.casts.astype(np.uint32)], axis=1).astype(np.uint32)
+    inst = dict(model=instances.model, rows=instances.rows, mesh=instances.mesh, aux=aux)
+    ms = [(m.positions, m.indices, 1 if (primitives and primitives[k]) else 0) for k, m in enumerate(meshes)]
+    return O.scene_words(layout, ms, inst, -1)
+
+
+def workload(config: int, engine, small: bool = False, pack=engine_pack, closest=gpu_closest) -> tuple:
+    """(Workload, uploaded scene). `closest(engine, scene, rays, mode)` traces the rays whose
+    hits spawn a step's secondary batches."""
     from renderlab_b200 import api as A
     from renderlab_b200 import scenes as S
-    primary = S.cluster_camera_rays(width, width)
-    dev = torch.from_numpy(primary).cuda()
-    h = engine.trace(scene, dev, A.CLOSEST, "plain")
-    torch.cuda.synchronize()
-    h = h.cpu().numpy().view(np.uint32)
-    hit = h[:, 1] != 0
-    t = h[hit, 0].view(np.float32)
-    pts = S.hit_points(primary[hit], t)
-    gi = S.hemisphere_rays(pts, S.triangle_normals(mesh, h[hit, 2]), primary[hit, 4:7], len(primary), S.Stream(0x5EED0002 + 1))
-    return primary, gi, float(hit.mean())
-
-
-def pick_kernel(name):
-    if name != "auto":
-        return name
-    from renderlab_b200 import api as A
-    return os.environ.get("RT_BENCH_KERNEL", "plain") if "plain" in A.KERNELS else "plain"
+    div = 4 if small else 1
+    if config == 1:
+        mesh = S.cubes_merged(100)
+        layout = A.LAYOUT_GI
+        words = pack(layout, [mesh], S.identity_instances(1), primitives=[True])
+        scene = engine.upload(layout, words)
+        w = 1024 // (2 if small else 1)
+        primary = S.cube_camera_rays(w, w)
+        hit, t, _ = _hits(layout, closest(engine, scene, primary, 0))
+        sun = S.sun_rays(S.hit_points(primary[hit], t[hit]))
+        return Workload(f"cubes-120k: 10,000 jittered unit cubes ({mesh.triangles:,} triangles) merged into one BLAS, "
+                        f"GI layout; {len(primary):,} primary closest-hit + {len(sun):,} sun any-hit rays per step",
+                        layout, words, [Batch("primary", primary, 0), Batch("sun", sun, 2)], [[0], [1]],
+                        mesh.triangles, dict(primary_hit_rate=float(hit.mean()))), scene
+    if config in (2, 3):
+        n_tris = (1_000_000 if config == 2 else 4_000_000) // div
+        mesh = S.clusters(n_tris, config=config)
+        layout = A.LAYOUT_REFLECTION
+        words = pack(layout, [mesh], S.identity_instances(1))
+        scene = engine.upload(layout, words)
+        if config == 2:
+            w = 2048 // (2 if small else 1)
+            primary = S.cluster_camera_rays(w, w)
+        else:
+            primary = S.cluster_camera_rays(4096 // (2 if small else 1), 2048 // (2 if small else 1))
+        hit, t, prim = _hits(layout, closest(engine, scene, primary, 0))
+        pts = S.hit_points(primary[hit], t[hit])
+        normals = S.triangle_normals(mesh, prim[hit])
+        if config == 2:
+            gi = S.hemisphere_rays(pts, normals, primary[hit, 4:7], len(primary), S.Stream(S.seed_for(2) + 1))
+            return Workload(f"clusters-1M: {mesh.triangles:,} triangles in clusters of 500 (reflection layout); "
+                            f"{len(primary):,} primary + {len(gi):,} GI hemisphere rays per step, closest hit",
+                            layout, words, [Batch("primary", primary, 0), Batch("gi", gi, 0)], [[0], [1]],
+                            mesh.triangles, dict(primary_hit_rate=float(hit.mean()))), scene
+        total = 2 * len(primary)
+        n_gi = (3 * total) // 10
+        n_sh = total - len(primary) - n_gi
+        gi = S.hemisphere_rays(pts, normals, primary[hit, 4:7], n_gi, S.Stream(S.seed_for(3) + 1))
+        shadow = S.point_light_rays(pts, normals, n_sh, 16, 100.0, S.Stream(S.seed_for(3) + 2))
+        return Workload(f"precision-4M: {mesh.triangles:,} cluster triangles (reflection layout); {total:,} rays per "
+                        f"step: {len(primary):,} primary, {len(gi):,} GI hemisphere (closest), {len(shadow):,} shadow "
+                        "any-hit toward 16 point lights", layout, words,
+                        [Batch("primary", primary, 0), Batch("gi", gi, 0), Batch("shadow", shadow, 2)],
+                        [[0], [1], [2]], mesh.triangles, dict(primary_hit_rate=float(hit.mean()))), scene
+    ms = S.multi_blas(n_instances=10_000 // div)
+    layout = A.LAYOUT_REFLECTION
+    words = pack(layout, ms.meshes, ms.instances)
+    scene = engine.upload(layout, words)
+    batches = [Batch(f"b{k}", r, m) for k, (r, m) in enumerate(S.uneven_batches(hi=2e6 / div))]
+    tris = sum(m.triangles for m in ms.meshes)
+    return Workload(f"batching: {len(ms.meshes)} BLAS ({tris:,} triangles, 2k-500k each) under {len(ms.instances):,} "
+                    f"rotated/scaled instances (reflection layout, TLAS); {len(batches)} batches of "
+                    f"{min(len(b.rays) for b in batches):,}-{max(len(b.rays) for b in batches):,} rays "
+                    f"({sum(len(b.rays) for b in batches):,} total, {sum(1 for b in batches if b.mode)} any-hit) "
+                    "in one persistent launch", layout, words, batches, [list(range(len(batches)))], tris,
+                    dict(instances=len(ms.instances))), scene
 
 
 # ---------------------------------------------------------------- measurement helpers
@@ -123,8 +225,9 @@ class Clocks:
         sm = np.array([float(r[2]) for r in rows])
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[6 + k].lower() == "active"})
+        power = [float(r[4]) for r in rows if r[4] not in ("", "[N/A]")]
         return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": float(rows[0][3]), "reasons": reasons,
-                "samples": len(rows), "power_w_max": max(float(r[4]) for r in rows if r[4] not in ("", "[N/A]"))}
+                "samples": len(rows), "power_w_max": max(power) if power else None}
 
 
 def _bus_of(pci: str):
@@ -143,35 +246,68 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-def bytes_per_ray(counters, n_rays, hit_bytes):
-    """Algorithmic bytes a ray reads/writes (reflection layout): ray 32 + hit + 128 per top
-    node + 96 per instance record + 64 per BLAS node + 48 per triangle tested."""
+def bvh4_bytes(counters, n_rays, layout, hit_bytes):
+    """Algorithmic bytes of the BVH4-Q8 walk: ray 32 + hit + 128 per top-level node + the
+    instance record per box test (GI 128, reflection 96) + 64 per BLAS node + 48 per triangle
+    (GI: 8 more per leaf for its index span)."""
     c = counters
-    total = (32 + hit_bytes) * n_rays + 128 * c["tlas_nodes"] + 96 * c["instance_box_tests"] \
-        + 64 * c["blas_nodes"] + 48 * c["triangle_tests"]
-    return total / n_rays
+    rec = 128 if layout == 0 else 96
+    return (32 + hit_bytes) * n_rays + 128 * c["tlas_nodes"] + rec * c["instance_box_tests"] \
+        + 64 * c["blas_nodes"] + 48 * c["triangle_tests"] + (8 * c["leaves"] if layout == 0 else 0)
 
 
-def cpu_baseline_leg(words, primary, gi, target_s, threads=None):
-    """The reference traversal (the oracle's restatement of rs_trace) on the host cores over a
-    strided sample of the step's rays; also returns its visit counters for the roofline."""
+def wide8_bytes(counters, layout, hit_bytes):
+    """The same for the 8-wide walk: 80 per node, 48 per triangle, 128 per top-level node, the
+    instance record (and 8 bytes of its 8-wide table) per instance test."""
+    c = counters
+    rec = (128 if layout == 0 else 96) + 8
+    return (32 + hit_bytes) * c["rays"] + 128 * c["top_nodes"] + rec * c["instance_tests"] + 80 * c["nodes"] \
+        + 48 * c["triangles"]
+
+
+def hit_bytes(layout, mode):
+    return 4 if mode else (40 if layout == 0 else 20)
+
+
+def oracle_trace(words, layout, rays, mode, counters=False, threads=None):
     from oracle import oracle as O
+    if layout == 0:
+        return O.gi_trace(words, rays, mode, counters=counters, threads=threads)
+    return O.rs_trace(words, rays, mode != 0, counters=counters, threads=threads)
+
+
+def sample_of(wl: Workload, n_total: int):
+    """A strided sample of every batch, n_total rays in proportion to the batch sizes."""
+    frac = min(1.0, n_total / max(1, wl.rays))
+    out = []
+    for b in wl.batches:
+        k = max(1, int(round(len(b.rays) * frac)))
+        stride = max(1, len(b.rays) // k)
+        out.append(b.rays[::stride][:k])
+    return out, frac
+
+
+def cpu_baseline_leg(wl: Workload, target_s: float, threads=None):
+    """The reference traversal (the oracle's restatement of the WGSL loop) on the host cores over
+    a strided sample of every batch of the step; also returns per-batch visit counters."""
     threads = threads or (os.cpu_count() or 1)
-    probe = np.concatenate([primary[::997][:4096], gi[::997][:4096]])
+    probe, _ = sample_of(wl, 4096)
     t0 = time.perf_counter()
-    O.rs_trace(words, probe, threads=threads)
-    per_ray = (time.perf_counter() - t0) / len(probe)
-    n_each = int(min(len(primary), max(4096, target_s / max(per_ray, 1e-9) / 2)))
-    stride = max(1, len(primary) // n_each)
-    sample = np.concatenate([primary[::stride][:n_each], gi[::stride][:n_each]])
+    for b, r in zip(wl.batches, probe):
+        oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
+    per_ray = (time.perf_counter() - t0) / sum(len(r) for r in probe)
+    sample, frac = sample_of(wl, int(max(4096, target_s / max(per_ray, 1e-9))))
+    n = sum(len(r) for r in sample)
     t0 = time.perf_counter()
-    O.rs_trace(words, sample, threads=threads)
+    for b, r in zip(wl.batches, sample):
+        oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
     wall = time.perf_counter() - t0
-    _, cp = O.rs_trace(words, primary[::stride][:n_each], counters=True, threads=threads)
-    _, cg = O.rs_trace(words, gi[::stride][:n_each], counters=True, threads=threads)
-    return dict(value=len(sample) / wall / 1e6, unit=UNIT, cores=threads, kind="port",
-                sample=f"{len(sample)} rays: every {stride}th primary and GI ray of the step, "
-                       f"oracle rs_trace (scalar f32 C++) on {threads} threads, {wall:.2f} s"), (cp, cg, n_each)
+    counts = [oracle_trace(wl.words, wl.layout, r, b.mode, counters=True, threads=threads)[1]
+              for b, r in zip(wl.batches, sample)]
+    return dict(value=n / wall / 1e6, unit=UNIT, cores=threads, kind="port",
+                sample=f"{n:,} rays ({100 * frac:.2f} % of each batch of the step, strided), oracle "
+                       f"{'gi_traverse' if wl.layout == 0 else 'rs_trace'} (scalar f32 C++) on {threads} threads, "
+                       f"{wall:.2f} s"), (counts, [len(r) for r in sample])
 
 
 # ---------------------------------------------------------------- arms
@@ -200,34 +336,44 @@ def max_over_ranks(x: float) -> float:
     return float(t.item())
 
 
+class HostScene:
+    """The reference arm's scene holder: it builds the workload without a GPU."""
+
+    def __init__(self):
+        self.layout, self.words = None, None
+
+    def upload(self, layout, words):
+        self.layout, self.words = layout, words
+        return self
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if int(os.environ.get("RANK", "0")) != 0:
         return  # rank 0 alone times the host-core reference
-    from oracle import oracle as O
-    from renderlab_b200 import scenes as S
-    mesh, words = make_scene(args.triangles)
-    primary = S.cluster_camera_rays(args.width, args.width)
-    hits, _ = O.rs_trace(words, primary[::64])  # GI rays from a sample of primary hits
-    hit = hits[:, 1] != 0
-    pts = S.hit_points(primary[::64][hit], hits[hit, 0].view(np.float32))
-    gi = S.hemisphere_rays(pts, S.triangle_normals(mesh, hits[hit, 2]), primary[::64][hit, 4:7], len(primary),
-                           S.Stream(0x5EED0002 + 1))
+    holder = HostScene()
+
+    def cpu_closest(engine, scene, rays, mode):
+        return oracle_trace(holder.words, holder.layout, rays, mode)[0]
+
+    wl, _ = workload(args.config, holder, args.small, pack=oracle_pack, closest=cpu_closest)
     threads = os.cpu_count() or 1
     per_step = max(1.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
     steps = []
     for k in range(args.warmup + args.steps):
-        base, _ = cpu_baseline_leg(words, primary, gi, per_step, threads)
+        base, _ = cpu_baseline_leg(wl, per_step, threads)
         if k >= args.warmup:
             steps.append(base)
     value = float(np.median([s["value"] for s in steps]))
-    cpu = dict(steps[-1])
-    cpu["value"] = value
+    cpu_line = dict(steps[-1])
+    cpu_line["value"] = value
     line = dict(metric=METRIC, value=value, unit=UNIT, impl="reference", n_gpus=world, steps=args.steps,
                 warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
-                data="synthetic", config=dict(workload=WORKLOAD, layout="reflection"), cpu_baseline=cpu,
-                e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
-                ms_per_step=None, note="oracle restatement of rs_trace: the Rust/WGSL reference cannot run here")
+                data="synthetic", config=dict(workload=wl.name, layout="GI" if wl.layout == 0 else "reflection",
+                                              config=args.config),
+                cpu_baseline=cpu_line, e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
+                ms_per_step=None, note="oracle restatement of the WGSL traversal loop on the host cores: the Rust/WGSL "
+                                       "reference cannot run here (no rustc, no Vulkan/wgpu)")
     print(json.dumps(line), flush=True)
 
 
@@ -236,118 +382,195 @@ def run_ours(args):
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
     from renderlab_b200 import api as A
-    kernel = pick_kernel(args.kernel)
+    from renderlab_b200 import tune as T
     engine = A.Engine(local)
-    if args.refill:
-        engine.set_tuning(fast_refill=args.refill, wide8_refill=args.refill)
-    mesh, words = make_scene(args.triangles)
-    scene = engine.upload(A.LAYOUT_REFLECTION, words)
+    wl, scene = workload(args.config, engine, args.small)
     t_prep = time.perf_counter()
-    scene.prepare(kernel)  # derived layouts (the 8-wide BVH) are scene-upload work, untimed
+    if args.kernel in ("auto", "wide8"):
+        scene.prepare("wide8")  # derived layouts (the 8-wide BVH) are scene-upload work, untimed
     t_prep = time.perf_counter() - t_prep
-    primary, gi, hit_rate = make_rays(engine, scene, mesh, args.width, kernel)
-    d_primary = torch.from_numpy(primary).cuda()
-    d_gi = torch.from_numpy(gi).cuda()
-    n_step = len(primary) + len(gi)
-    h_p = torch.empty((len(primary), 5), dtype=torch.int32, device="cuda")
-    h_g = torch.empty((len(gi), 5), dtype=torch.int32, device="cuda")
+    dev = [torch.from_numpy(b.rays).cuda() for b in wl.batches]
+
+    def hit_tensor(b):
+        words = A.hit_words(wl.layout, b.mode)
+        return torch.empty((len(b.rays), words) if words > 1 else (len(b.rays),), dtype=torch.int32, device="cuda")
+
+    plain_hits = [hit_tensor(b) for b in wl.batches]
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     stream = torch.cuda.current_stream()
 
-    def step():
-        engine.trace(scene, d_primary, A.CLOSEST, kernel, hits=h_p)
-        engine.trace(scene, d_gi, A.CLOSEST, kernel, hits=h_g)
+    # ---- product plans: one per group, from the autotuner (or the forced kernel)
+    t_tune = time.perf_counter()
+    plans, tables = [], []
+    for g in wl.groups:
+        batches = [(dev[i], wl.batches[i].mode) for i in g]
+        if args.kernel == "auto":
+            heavy = len(g) > 8  # the many-batch launch runs for seconds: one timed launch a candidate
+            ch = T.tune(engine, scene, batches, flush=flush, reps=1 if heavy else 3, max_seconds=20.0)
+            plans.append(ch.plan)
+            tables.append(ch.table()[:6])
+        elif args.kernel == "plain":
+            plans.append(None)
+        else:
+            plans.append(engine.plan(scene, batches, args.kernel, refill=args.refill, order=args.order))
+    t_tune = time.perf_counter() - t_tune
+
+    def plain_step():
+        for i, b in enumerate(wl.batches):
+            engine.trace(scene, dev[i], b.mode, "plain", hits=plain_hits[i])
+
+    def product_step(evs=None):
+        for k, (g, p) in enumerate(zip(wl.groups, plans)):
+            if evs is not None:
+                evs[k].record(stream)
+            if p is None:
+                for i in g:
+                    engine.trace(scene, dev[i], wl.batches[i].mode, "plain", hits=plain_hits[i])
+            else:
+                p.launch()
+        if evs is not None:
+            evs[-1].record(stream)
 
     for _ in range(max(3, args.warmup)):
         flush.zero_()
-        step()
+        plain_step()
+        flush.zero_()
+        product_step()
     torch.cuda.synchronize()
-    # matched hits: the kernel under test against the plain kernel on this step's rays
-    ref_p = engine.trace(scene, d_primary, A.CLOSEST, "plain").cpu().numpy()
-    ref_g = engine.trace(scene, d_gi, A.CLOSEST, "plain").cpu().numpy()
-    matched = float(((h_p.cpu().numpy()[:, 1:3] == ref_p[:, 1:3]).all(1).sum()
-                     + (h_g.cpu().numpy()[:, 1:3] == ref_g[:, 1:3]).all(1).sum()) / n_step)
+    # matched hits: product results against the plain kernel's, per ray (ids, or the any-hit flag)
+    matched, n_all = 0, 0
+    for g, p in zip(wl.groups, plans):
+        for j, i in enumerate(g):
+            ref = plain_hits[i]
+            got = p.hits[j] if p is not None else ref
+            if ref.dim() == 2:
+                cols = slice(1, 3) if wl.layout == A.LAYOUT_REFLECTION else slice(1, 5)
+                same = (got[:, cols] == ref[:, cols]).all(1)
+            else:
+                same = got == ref
+            matched += int(same.sum().item())
+            n_all += ref.shape[0]
 
     bus = None
     try:
         bus = torch.cuda.get_device_properties(local).pci_bus_id
     except AttributeError:
         pass
+
+    def timed(fn_step, groups):
+        evs = [[torch.cuda.Event(enable_timing=True) for _ in range(groups + 1)] for _ in range(args.steps)]
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        for k in range(args.steps):
+            flush.zero_()
+            fn_step(evs[k])
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+        return np.array([[evs[k][j].elapsed_time(evs[k][j + 1]) for j in range(groups)] for k in range(args.steps)])
+
+    def plain_timed(evs):
+        evs[0].record(stream)
+        plain_step()
+        evs[1].record(stream)
+
     clocks = Clocks()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-          for _ in range(args.steps)]
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
     clocks.start()
     wall0 = time.perf_counter()
-    for k in range(args.steps):
-        flush.zero_()
-        ev[k][0].record(stream)
-        engine.trace(scene, d_primary, A.CLOSEST, kernel, hits=h_p)
-        ev[k][1].record(stream)
-        engine.trace(scene, d_gi, A.CLOSEST, kernel, hits=h_g)
-        ev[k][2].record(stream)
-    torch.cuda.synchronize()
+    prod_ms = timed(product_step, len(wl.groups))
+    plain_ms = timed(plain_timed, 1)
     wall = time.perf_counter() - wall0
-    if world > 1:
-        torch.distributed.barrier()
     clk = clocks.stop(bus)
-    prim_ms = np.array([a.elapsed_time(b) for a, b, _ in ev])
-    gi_ms = np.array([b.elapsed_time(c) for _, b, c in ev])
-    step_ms = prim_ms + gi_ms
+    step_ms = prod_ms.sum(1)
     ms = float(step_ms.mean())
+    ms_plain = float(plain_ms.sum(1).mean())
     if world > 1:
-        ms = max_over_ranks(ms)
+        ms, ms_plain = max_over_ranks(ms), max_over_ranks(ms_plain)
+    n_step = wl.rays
     value = world * n_step / (ms * 1e-3) / 1e6
+    plain_value = world * n_step / (ms_plain * 1e-3) / 1e6
 
-    # e2e through the host-buffer C ABI call: pinned rays in, hits out, copies inside the timing
-    hp = torch.from_numpy(primary).pin_memory()
-    hg = torch.from_numpy(gi).pin_memory()
-    op = torch.empty((len(primary), 5), dtype=torch.int32).pin_memory()
-    og = torch.empty((len(gi), 5), dtype=torch.int32).pin_memory()
-    engine.reserve(len(primary))
-    for _ in range(2):
-        engine.trace_host(scene, hp, A.CLOSEST, kernel, out=op)
+    # e2e through the host-buffer C ABI call, with each group's kernel and wavefront width
+    pinned = [torch.from_numpy(b.rays).pin_memory() for b in wl.batches]
+    outs = [torch.empty(tuple(h.shape), dtype=torch.int32).pin_memory() for h in plain_hits]
+    engine.reserve(min(max(len(b.rays) for b in wl.batches), 1 << 22))
+
+    def host_step():
+        for g, p in zip(wl.groups, plans):
+            kern = p.desc["kernel"] if p is not None else "plain"
+            if p is not None:
+                engine.set_tuning(**{f"{kern}_refill": p.desc["refill"] or 8})
+            for i in g:
+                engine.trace_host(scene, pinned[i], wl.batches[i].mode, kern, out=outs[i])
+
+    host_step()
     e2e_steps = max(3, min(args.steps, 10))
     t0 = time.perf_counter()
     for _ in range(e2e_steps):
-        engine.trace_host(scene, hp, A.CLOSEST, kernel, out=op)
-        engine.trace_host(scene, hg, A.CLOSEST, kernel, out=og)
+        host_step()
     e2e_s = (time.perf_counter() - t0) / e2e_steps
     if world > 1:
         e2e_s = max_over_ranks(e2e_s)
     e2e = dict(value=world * n_step / e2e_s / 1e6, unit=UNIT, h2d_bytes_per_step=n_step * 32,
-               d2h_bytes_per_step=n_step * 20, ms_per_step=e2e_s * 1e3)
+               d2h_bytes_per_step=int(sum(len(b.rays) * hit_bytes(wl.layout, b.mode) for b in wl.batches)),
+               ms_per_step=e2e_s * 1e3, path="rt_trace_host (pinned host rays in, host hits out)")
 
     if rank != 0:
         return
     cpu, counts = (None, None)
     if not args.no_cpu:
-        cpu, counts = cpu_baseline_leg(words, primary, gi, args.cpu_seconds)
+        cpu, counts = cpu_baseline_leg(wl, args.cpu_seconds)
     peak, peak_kind = measured_peak()
     roof = None
-    if counts:
-        cp, cg, n_each = counts
-        bp, bg = bytes_per_ray(cp, n_each, 20), bytes_per_ray(cg, n_each, 20)
-        alg_bytes = bp * len(primary) + bg * len(gi)
-        achieved = alg_bytes / (ms * 1e-3) / 1e9
-        roof = dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
-                    traffic=None, peak_source=f"{peak_kind} hbm_gbs",
-                    bytes_per_ray=dict(primary=bp, gi=bg), roofline_mrays=peak * 1e9 / ((alg_bytes / n_step)) / 1e6,
-                    note="scene (51 MB) is L2-resident: algorithmic bytes over the HBM peak may exceed 1")
+    alg = 0.0
+    notes = []
+    for g, p in zip(wl.groups, plans):
+        kern = p.desc["kernel"] if p is not None else "plain"
+        for i in g:
+            b = wl.batches[i]
+            hb = hit_bytes(wl.layout, b.mode)
+            if kern == "wide8":  # the 8-wide walk's visit counters on every 16th ray
+                c = engine.trace_counted(scene, dev[i][::16].contiguous(), b.mode, "wide8")
+                alg += wide8_bytes(c, wl.layout, hb) * len(b.rays) / max(1, c["rays"])
+            elif counts is not None:
+                cnt, nsamp = counts
+                alg += bvh4_bytes(cnt[i], nsamp[i], wl.layout, hb) * len(b.rays) / max(1, nsamp[i])
+            else:
+                notes.append("no oracle counters (--no-cpu): BVH4 bytes not counted")
+    if alg > 0:
+        achieved = alg / (ms * 1e-3) / 1e9
+        roof = dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak, traffic=None,
+                    peak_source=f"{peak_kind} hbm_gbs", bytes_per_ray=alg / n_step,
+                    roofline_mrays=peak * 1e9 / (alg / n_step) / 1e6,
+                    note="algorithmic bytes of the chosen kernels' walks (visit counters) over the product time; "
+                         "scenes under 126 MB are L2-resident, so the HBM fraction is a ceiling check, not the limit")
+    launches_per_step = sum((1 + (1 if p.desc["order"] != "none" else 0)) if p is not None else len(g)
+                            for g, p in zip(wl.groups, plans))
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
         higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
-        config=dict(workload=WORKLOAD, kernel=kernel, layout="reflection", triangles=args.triangles,
-                    rays_per_step=n_step, primary_hit_rate=hit_rate, prepare_s=t_prep, l2="flushed before each step (256 MiB write)",
-                    parallelism=f"replicas x{world}"),
-        latency_ms=dict(p50=float(np.percentile(step_ms, 50)), p99=float(np.percentile(step_ms, 99))),
-        breakdown=dict(primary_mrays=float(len(primary) / (prim_ms.mean() * 1e-3) / 1e6),
-                       gi_mrays=float(len(gi) / (gi_ms.mean() * 1e-3) / 1e6)),
-        matched_hits_vs_plain=matched, wall_s=wall,
-        roofline=roof, cpu_baseline=cpu, clocks=clk, e2e=e2e, gpu_launches=2 * args.steps)
+        config=dict(workload=wl.name, config=args.config, layout="GI" if wl.layout == 0 else "reflection",
+                    triangles=wl.triangles, rays_per_step=n_step, l2="flushed before each step (256 MiB write)",
+                    parallelism=f"replicas x{world}", prepare_s=t_prep, tune_s=t_tune, **wl.info,
+                    plans=[p.desc if p is not None else {"kernel": "plain"} for p in plans]),
+        plain=dict(value=plain_value, ms_per_step=ms_plain, launches_per_step=len(wl.batches)),
+        speedup_vs_plain=value / plain_value,
+        matched_hits_vs_plain=matched / max(1, n_all),
+        latency_ms=dict(p50=float(np.percentile(step_ms, 50)), p99=float(np.percentile(step_ms, 99)),
+                        plain_p50=float(np.percentile(plain_ms.sum(1), 50)),
+                        plain_p99=float(np.percentile(plain_ms.sum(1), 99))),
+        breakdown={("+".join(wl.batches[i].label for i in g) if len(g) <= 3 else f"{len(g)} batches"):
+                   float(sum(len(wl.batches[i].rays) for i in g) / (prod_ms[:, k].mean() * 1e-3) / 1e6)
+                   for k, g in enumerate(wl.groups)},
+        tuning=tables, wall_s=wall,
+        roofline=roof, cpu_baseline=cpu, clocks=clk, e2e=e2e, gpu_launches=launches_per_step * args.steps)
+    if notes:
+        line["notes"] = sorted(set(notes))
     print(json.dumps(line), flush=True)
+    for p in plans:
+        if p is not None:
+            p.close()
     scene.release()
     engine.close()
 

@@ -190,6 +190,58 @@ def clusters(n_triangles: int, config: int = 2, per_cluster: int = 500, half: fl
     return Mesh(pos, np.arange(3 * n_triangles, dtype=np.uint32))
 
 
+def quaternion_matrices(s: Stream, n: int) -> np.ndarray:
+    """Uniformly random rotations (Shoemake's subgroup algorithm), (n, 3, 3) float64."""
+    u = s.uniform(n, 3)
+    a, b = np.sqrt(1.0 - u[:, 0]), np.sqrt(u[:, 0])
+    t1, t2 = 2.0 * np.pi * u[:, 1], 2.0 * np.pi * u[:, 2]
+    x, y, z, w = a * np.sin(t1), a * np.cos(t1), b * np.sin(t2), b * np.cos(t2)
+    return np.stack([
+        np.stack([1 - 2 * (y * y + z * z), 2 * (x * y - z * w), 2 * (x * z + y * w)], axis=1),
+        np.stack([2 * (x * y + z * w), 1 - 2 * (x * x + z * z), 2 * (y * z - x * w)], axis=1),
+        np.stack([2 * (x * z - y * w), 2 * (y * z + x * w), 1 - 2 * (x * x + y * y)], axis=1),
+    ], axis=1)
+
+
+@dataclass
+class MultiScene:
+    meshes: list       # Mesh per BLAS
+    instances: Instances
+    half: float        # instances' translations lie in [-half, half]^3
+
+
+def multi_blas(n_blas: int = 64, n_instances: int = 10_000, tri_lo: float = 2e3, tri_hi: float = 5e5,
+               half: float = 500.0, scale=(0.5, 4.0), config: int = 4) -> MultiScene:
+    """Config 4 / 5 scenes: n_blas cluster meshes with log-uniform triangle counts, under
+    n_instances instances with uniform random rotations, uniform scales and translations in
+    [-half, half]^3; each instance picks its BLAS uniformly."""
+    s = Stream(seed_for(config))
+    counts = np.round(np.exp(s.range(np.log(tri_lo), np.log(tri_hi), n_blas))).astype(np.int64)
+    meshes = [clusters(int(c), stream=Stream(seed_for(config) ^ (0x9E37 * (k + 1)))) for k, c in enumerate(counts)]
+    which = np.minimum((s.uniform(n_instances) * n_blas).astype(np.int64), n_blas - 1).astype(np.uint32)
+    rot = quaternion_matrices(s, n_instances)
+    sc = s.range(scale[0], scale[1], n_instances)
+    tr = s.range(-half, half, n_instances, 3)
+    model = np.concatenate([rot * sc[:, None, None], tr[:, :, None]], axis=2).astype(np.float32)
+    return MultiScene(meshes, Instances(model, affine_inverse_rows(model), which), half)
+
+
+def uneven_batches(n_batches: int = 64, lo: float = 1e3, hi: float = 2e6, half: float = 500.0, config: int = 4,
+                   tmax: float = 1e30):
+    """Config 4 ray batches: sizes log-uniform in [lo, hi], closest / any hit by a fair coin per
+    batch, origins uniform in [-half, half]^3, directions uniform on the sphere. Returns a list
+    of (rays, mode) with mode 0 closest, 2 any hit (casters within tmax)."""
+    s = Stream(seed_for(config) + 0x100)
+    sizes = np.round(np.exp(s.range(np.log(lo), np.log(hi), n_batches))).astype(np.int64)
+    coins = s.uniform(n_batches) < 0.5
+    out = []
+    for n, any_hit in zip(sizes, coins):
+        o = s.range(-half, half, int(n), 3)
+        d = s.unit_vectors(int(n))
+        out.append((pack_rays(o, d, 0.0, tmax), 2 if any_hit else 0))
+    return out
+
+
 # ---------------------------------------------------------------- rays
 
 RAY_DTYPE = np.dtype([("o", np.float32, 3), ("tmin", np.float32), ("d", np.float32, 3), ("tmax", np.float32)])
@@ -273,6 +325,19 @@ def hemisphere_rays(points: np.ndarray, normals: np.ndarray, incoming: np.ndarra
     b = np.cross(n, t)
     d = t * lx[:, None] + b * ly[:, None] + n * lz[:, None]
     return pack_rays(p, d, offset_tmin(p), tmax)
+
+
+def point_light_rays(points: np.ndarray, normals: np.ndarray, count: int, n_lights: int, half: float,
+                     stream: Stream) -> np.ndarray:
+    """Config 3 shadow rays: from the given hit points taken in turn toward one of n_lights point
+    lights uniform in [-half, half]^3 (chosen uniformly), tmax = distance * (1 - 1e-4)."""
+    lights = stream.range(-half, half, n_lights, 3)
+    k = np.arange(count) % len(points)
+    p = points[k].astype(np.float64)
+    which = np.minimum((stream.uniform(count) * n_lights).astype(np.int64), n_lights - 1)
+    v = lights[which] - p
+    dist = np.maximum(np.linalg.norm(v, axis=1), 1e-30)
+    return pack_rays(p, v / dist[:, None], offset_tmin(p), dist * (1.0 - 1e-4))
 
 
 def hit_points(rays: np.ndarray, t: np.ndarray) -> np.ndarray:

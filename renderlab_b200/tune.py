@@ -1,0 +1,120 @@
+"""The autotuner: picks, per scene and per batch set, the launch parameters of the persistent
+traversal by timing candidate plans on the device.
+
+Parameters searched (each candidate is one rt_plan, timed as a whole, sort included):
+
+* kernel -- FAST (BVH4-Q8, bit-exact with the reference loop) or WIDE8 (8-wide compressed
+  nodes, watertight f32 test with f64 re-tests);
+* wavefront width -- the refill threshold: how many lanes of a 32-wide warp must be idle before
+  the warp takes more rays (1 keeps every lane busy; 32 hands out whole runs of 32 consecutive
+  rays, which keeps a coherent batch's 8 x 4 tiles together);
+* sort key -- none, or a ray permutation by origin Morton code / octant + origin (rt_order_rays
+  over the plan's whole ray space, run inside the plan on every launch).
+
+Stack depth is not a free parameter: the bit-exact kernels keep the reference's 48-entry stack
+(gi_rays_software.wgsl:22, reflections_software_bvh4.wgsl:12), whose overflow behaviour is part
+of their results, and WIDE8 a 32-entry node-group stack (one entry per level of the 8-wide tree).
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import api as A
+
+KERNELS = ("fast", "wide8")
+REFILLS = (4, 8, 16, 32)
+ORDERS = ("none", "origin", "octant")
+
+
+@dataclass
+class Trial:
+    kernel: str
+    refill: int
+    order: str
+    ms: float
+    mrays: float
+
+
+@dataclass
+class Choice:
+    plan: A.Plan
+    trials: list = field(default_factory=list)
+
+    @property
+    def best(self) -> Trial:
+        return min(self.trials, key=lambda t: t.ms)
+
+    def table(self) -> list:
+        return [dict(kernel=t.kernel, refill=t.refill, order=t.order, ms=round(t.ms, 4), mrays=round(t.mrays, 1))
+                for t in sorted(self.trials, key=lambda t: t.ms)]
+
+
+def time_plan(plan: A.Plan, reps: int = 3, warmup: int = 1, flush=None) -> float:
+    """Median device time (ms) of `reps` launches after `warmup` untimed ones; `flush` (a CUDA
+    byte tensor larger than L2) is rewritten before every timed launch when given."""
+    import torch
+    for _ in range(warmup):
+        plan.launch()
+    times = []
+    for _ in range(reps):
+        if flush is not None:
+            flush.zero_()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        plan.launch()
+        b.record()
+        torch.cuda.synchronize()
+        times.append(a.elapsed_time(b))
+    return float(np.median(times))
+
+
+def candidates(kernels=KERNELS, refills=REFILLS, orders=ORDERS) -> list:
+    """Every (kernel, refill, order), the usual winners first: unsorted before sorted, the middle
+    and widest wavefronts before the rest."""
+    pri = {8: 0, 32: 1, 16: 2, 4: 3}
+    return sorted(((k, r, o) for k in kernels for r in refills for o in orders),
+                  key=lambda c: (orders.index(c[2]) > 0, pri.get(c[1], 4), kernels.index(c[0])))
+
+
+def tune(engine: A.Engine, scene: A.Scene, batches, kernels=KERNELS, refills=REFILLS, orders=ORDERS,
+         graph: bool = True, reps: int = 3, flush=None, max_seconds: float = 30.0) -> Choice:
+    """Times (kernel, refill, order) plans over `batches` ((rays, mode[, hits]) on the device),
+    in candidates() order until all are timed or `max_seconds` of device time is spent, and
+    returns the fastest plan, built and ready to launch, with the trial table. WIDE8 candidates
+    are skipped unless the scene has been prepared for WIDE8."""
+    import torch
+    rays = sum(int(b[0].shape[0]) for b in batches)
+    with_hits = []  # one set of hit buffers, shared by every candidate plan
+    for b in batches:
+        r, mode = b[0], b[1]
+        h = b[2] if len(b) > 2 and b[2] is not None else None
+        if h is None:
+            words = A.hit_words(scene.layout, mode)
+            n = int(r.shape[0])
+            h = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=r.device)
+        with_hits.append((r, mode, h))
+    best_plan, best_ms, trials, spent, skip = None, None, [], 0.0, set()
+    for kernel, refill, order in candidates(kernels, refills, orders):
+        if kernel in skip:
+            continue
+        if trials and spent > max_seconds:
+            break
+        try:
+            plan = engine.plan(scene, with_hits, kernel, refill=refill, order=order, graph=graph)
+        except A.RtError as e:
+            if "UNSUPPORTED" in str(e):
+                skip.add(kernel)
+                continue
+            raise
+        ms = time_plan(plan, reps=reps, flush=flush)
+        spent += ms * (reps + 1) * 1e-3
+        trials.append(Trial(kernel, refill, order, ms, rays / (ms * 1e-3) / 1e6 if ms > 0 else 0.0))
+        if best_ms is None or ms < best_ms:
+            if best_plan is not None:
+                best_plan.close()
+            best_plan, best_ms = plan, ms
+        else:
+            plan.close()
+    return Choice(best_plan, trials)

@@ -83,3 +83,10 @@ def test_validation_rejects_unsafe_words():
         pass
     else:
         raise AssertionError("cycle accepted")
+
+
+def test_tuner_candidates_cover_the_grid_once():
+    from renderlab_b200 import tune as T
+    c = T.candidates()
+    assert len(c) == len(set(c)) == len(T.KERNELS) * len(T.REFILLS) * len(T.ORDERS)
+    assert c[0][2] == "none" and c[-1][2] != "none"

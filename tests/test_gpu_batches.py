@@ -140,3 +140,31 @@ def test_batch_rejections(engine):
         assert engine.trace_batches(scene, [], "fast") == []
     finally:
         scene.release()
+
+
+def test_tuner_plan_matches_plain(engine):
+    """The autotuner's chosen plan (WIDE8 allowed) gives the plain kernel's hits, near ties
+    aside, and its trial table covers both kernels."""
+    from renderlab_b200 import tune as T
+    torch = _torch()
+    words, batches = _scene_and_batches(A.LAYOUT_REFLECTION)
+    scene = engine.upload(A.LAYOUT_REFLECTION, words)
+    try:
+        scene.prepare("wide8")
+        dev = _device(batches)
+        ch = T.tune(engine, scene, dev, refills=(8, 32), orders=("none", "octant"), reps=1)
+        assert {t.kernel for t in ch.trials} == {"fast", "wide8"} and len(ch.trials) == 8
+        ch.plan.launch()
+        torch.cuda.synchronize()
+        plain = _alone(engine, scene, dev, "plain")
+        for g, w in zip(ch.plan.hits, plain):
+            if w is None:
+                continue
+            if w.dim() == 2:
+                same = (g[:, 1:3] == w[:, 1:3]).all(1).float().mean().item()
+            else:
+                same = (g == w).float().mean().item()
+            assert same >= 0.999, same
+        ch.plan.close()
+    finally:
+        scene.release()
