@@ -499,7 +499,7 @@ def run_ours(args):
     def host_step():
         for g, p in zip(wl.groups, plans):
             kern = p.desc["kernel"] if p is not None else "plain"
-            if p is not None:
+            if kern != "plain":
                 engine.set_tuning(**{f"{kern}_refill": p.desc["refill"] or 8})
             for i in g:
                 engine.trace_host(scene, pinned[i], wl.batches[i].mode, kern, out=outs[i])
@@ -545,8 +545,12 @@ def run_ours(args):
                     roofline_mrays=peak * 1e9 / (alg / n_step) / 1e6,
                     note="algorithmic bytes of the chosen kernels' walks (visit counters) over the product time; "
                          "scenes under 126 MB are L2-resident, so the HBM fraction is a ceiling check, not the limit")
-    launches_per_step = sum((1 + (1 if p.desc["order"] != "none" else 0)) if p is not None else len(g)
-                            for g, p in zip(wl.groups, plans))
+    def launches(g, p):  # traversal kernels (and ray-key kernels) a step launches
+        if p is None or p.desc["kernel"] == "plain":
+            return sum(1 for i in g if len(wl.batches[i].rays))
+        return 1 + (1 if p.desc["order"] != "none" else 0)
+
+    launches_per_step = sum(launches(g, p) for g, p in zip(wl.groups, plans))
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
         higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",

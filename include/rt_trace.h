@@ -176,7 +176,9 @@ typedef struct rt_batch {
 } rt_batch;
 #define RT_MAX_BATCHES 4096u
 /* Stream-ordered; the batch table is staged through the context (h_batches may be reused on
- * return). kernel: RT_KERNEL_FAST or RT_KERNEL_WIDE8. At most RT_MAX_BATCHES batches. */
+ * return). kernel: RT_KERNEL_FAST or RT_KERNEL_WIDE8 (one persistent launch), or RT_KERNEL_PLAIN
+ * (one launch per batch, for comparison and for workloads too short to fill a persistent grid).
+ * At most RT_MAX_BATCHES batches. */
 rt_status rt_trace_batches(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const rt_batch* h_batches,
                            uint32_t n_batches, void* stream);
 
@@ -187,9 +189,9 @@ rt_status rt_trace_batches(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel,
  * counter): issue them on one stream. */
 typedef struct rt_plan rt_plan;
 typedef struct rt_plan_desc {
-  rt_kernel kernel;   /* RT_KERNEL_FAST or RT_KERNEL_WIDE8 */
+  rt_kernel kernel;   /* RT_KERNEL_FAST or RT_KERNEL_WIDE8; RT_KERNEL_PLAIN: a launch per batch */
   uint32_t refill;    /* idle lanes (1-32) before a warp takes more rays; 0: the context's tuning */
-  rt_ray_order order; /* sort the launch's rays first (RT_ORDER_NONE: no sort) */
+  rt_ray_order order; /* sort the launch's rays first (RT_ORDER_NONE: no sort; PLAIN takes none) */
   uint32_t graph;     /* 1: replay a captured CUDA graph; 0: launch directly */
 } rt_plan_desc;
 rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_batches, uint32_t n_batches,

@@ -14,17 +14,19 @@ namespace {
 
 constexpr uint64_t MAX_LAUNCH_RAYS = 1ull << 31;  // the ray counter's headroom stays below 2^32
 
-// Checks the batches and fills the device-format table; total receives the launch's rays.
+// Checks the batches and fills the device-format table; total receives the launch's rays and
+// uniform the shared mode of its non-empty batches (0 closest, 1 any hit, -1 mixed).
 rt_status make_table(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const rt_batch* b, uint32_t n,
-                     rtk::BatchEntry* table, uint64_t& total) {
+                     rtk::BatchEntry* table, uint64_t& total, int& uniform) {
   if (!scene) return fail(ctx, RT_ERR_INVALID_ARG, "null scene");
-  if (kernel != RT_KERNEL_FAST && kernel != RT_KERNEL_WIDE8)
-    return fail(ctx, RT_ERR_UNSUPPORTED, "many-batch launches run the FAST or WIDE8 kernel");
+  if (kernel != RT_KERNEL_PLAIN && kernel != RT_KERNEL_FAST && kernel != RT_KERNEL_WIDE8)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
   if (kernel == RT_KERNEL_WIDE8 && !scene->d_wide8)
     return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
   if (n && !b) return fail(ctx, RT_ERR_INVALID_ARG, "null batch array");
   if (n > RT_MAX_BATCHES) return fail(ctx, RT_ERR_INVALID_ARG, "%u batches (at most %u)", n, RT_MAX_BATCHES);
   total = 0;
+  uniform = -2;  // no non-empty batch yet
   for (uint32_t i = 0; i < n; ++i) {
     if ((unsigned)b[i].mode > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "batch %u: unknown mode %d", i, (int)b[i].mode);
     if (b[i].n) {
@@ -42,17 +44,34 @@ rt_status make_table(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const
     table[i].pad = 0;
     total += b[i].n;
     if (total > MAX_LAUNCH_RAYS) return fail(ctx, RT_ERR_INVALID_ARG, "more than 2^31 rays in one launch");
+    if (b[i].n) {
+      const int m = b[i].mode != RT_CLOSEST ? 1 : 0;
+      uniform = uniform == -2 ? m : (uniform == m ? m : -1);
+    }
   }
+  if (uniform == -2) uniform = 0;
   return RT_OK;
+}
+
+// The PLAIN kernel has no ray queue: one launch per non-empty batch, from the host table.
+cudaError_t enqueue_plain(const rt_scene* scene, const rtk::BatchEntry* h_table, uint32_t entries, rtk::DevStatus* st,
+                          cudaStream_t s) {
+  const rtl::SceneView v = view_of(scene);
+  for (uint32_t i = 0; i < entries; ++i) {
+    if (!h_table[i].n) continue;
+    cudaError_t e = rtl::launch_plain(v, h_table[i].mode, h_table[i].rays, h_table[i].hits, h_table[i].n, st, s);
+    if (e != cudaSuccess) return e;
+  }
+  return cudaSuccess;
 }
 
 cudaError_t enqueue(const rt_scene* scene, rt_kernel kernel, const rtk::BatchEntry* d_table, uint32_t entries,
                     uint32_t total, const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t s,
-                    uint32_t refill) {
+                    uint32_t refill, int uniform) {
   const rtl::SceneView v = view_of(scene);
   if (kernel == RT_KERNEL_WIDE8)
-    return rtl::launch_wide8_batches(v, d_table, entries, total, order, counter, st, s, refill);
-  return rtl::launch_fast_batches(v, d_table, entries, total, order, counter, st, s, refill);
+    return rtl::launch_wide8_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform);
+  return rtl::launch_fast_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform);
 }
 
 void world_box(const rt_scene* scene, float lo[3], float hi[3]) {
@@ -85,14 +104,22 @@ rt_status rt_trace_batches(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel,
   rtk::BatchEntry* h = ctx->h_tables + (size_t)slot * RT_MAX_BATCHES;
   rtk::BatchEntry* d = ctx->d_tables + (size_t)slot * RT_MAX_BATCHES;
   uint64_t total = 0;
-  rt_status st = make_table(ctx, scene, kernel, h_batches, n_batches, h, total);
+  int uniform = -1;
+  rt_status st = make_table(ctx, scene, kernel, h_batches, n_batches, h, total, uniform);
   if (st != RT_OK || total == 0) return st;
   cudaStream_t s = static_cast<cudaStream_t>(stream);
+  if (kernel == RT_KERNEL_PLAIN) {
+    cudaError_t e = enqueue_plain(scene, h, n_batches, ctx->d_status, s);
+    if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "plain batch launch: %s", cudaGetErrorString(e));
+    ctx->rays += total;
+    ctx->launches += n_batches;
+    return RT_OK;
+  }
   RT_CUDA(ctx, cudaMemcpyAsync(d, h, sizeof(rtk::BatchEntry) * n_batches, cudaMemcpyHostToDevice, s));
   RT_CUDA(ctx, cudaEventRecord(ctx->table_done[slot], s));
   const uint32_t refill = kernel == RT_KERNEL_WIDE8 ? ctx->tuning.wide8_refill : ctx->tuning.fast_refill;
   cudaError_t e = enqueue(scene, kernel, d, n_batches, (uint32_t)total, nullptr,
-                          ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, s, refill);
+                          ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, s, refill, uniform);
   if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "many-batch launch: %s", cudaGetErrorString(e));
   ctx->rays += total;
   ctx->launches += 1;
@@ -104,6 +131,7 @@ struct rt_plan {
   const rt_scene* scene = nullptr;
   rt_plan_desc desc{};
   uint32_t entries = 0, total = 0, refill = 8;
+  int uniform = -1;
   rtk::BatchEntry* d_table = nullptr;
   unsigned int* d_counter = nullptr;
   uint32_t* d_order = nullptr;
@@ -111,6 +139,7 @@ struct rt_plan {
   size_t sort_bytes = 0;
   size_t device_bytes = 0;
   float lo[3] = {}, hi[3] = {};
+  std::vector<rtk::BatchEntry> h_table;  // the PLAIN kernel's launches read it
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
 };
@@ -119,13 +148,14 @@ namespace {
 
 cudaError_t plan_enqueue(const rt_plan* p, cudaStream_t s) {
   if (p->total == 0) return cudaSuccess;
+  if (p->desc.kernel == RT_KERNEL_PLAIN) return enqueue_plain(p->scene, p->h_table.data(), p->entries, p->ctx->d_status, s);
   if (p->d_order) {
     cudaError_t e = rtl::launch_order_batches(p->d_table, p->entries, p->total, p->lo, p->hi, (uint32_t)p->desc.order,
                                               p->d_order, p->d_sort, p->sort_bytes, s);
     if (e != cudaSuccess) return e;
   }
   return enqueue(p->scene, p->desc.kernel, p->d_table, p->entries, p->total, p->d_order, p->d_counter,
-                 p->ctx->d_status, s, p->refill);
+                 p->ctx->d_status, s, p->refill, p->uniform);
 }
 
 void plan_free(rt_plan* p) {
@@ -146,9 +176,12 @@ rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_b
   *out = nullptr;
   if ((unsigned)desc->order > 3u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown ray order %d", (int)desc->order);
   if (desc->refill > 32) return fail(ctx, RT_ERR_INVALID_ARG, "refill thresholds are 1-32 lanes");
+  if (desc->kernel == RT_KERNEL_PLAIN && desc->order != RT_ORDER_NONE)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the PLAIN kernel takes no ray order");
   std::vector<rtk::BatchEntry> table(n_batches ? n_batches : 1);
   uint64_t total = 0;
-  rt_status st = make_table(ctx, scene, desc->kernel, h_batches, n_batches, table.data(), total);
+  int uniform = -1;
+  rt_status st = make_table(ctx, scene, desc->kernel, h_batches, n_batches, table.data(), total, uniform);
   if (st != RT_OK) return st;
   RT_CUDA(ctx, cudaSetDevice(ctx->device));
   rt_plan* p = new rt_plan;
@@ -157,6 +190,8 @@ rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_b
   p->desc = *desc;
   p->entries = n_batches;
   p->total = (uint32_t)total;
+  p->uniform = uniform;
+  p->h_table = table;
   p->refill = desc->refill ? desc->refill
                            : (desc->kernel == RT_KERNEL_WIDE8 ? ctx->tuning.wide8_refill : ctx->tuning.fast_refill);
   world_box(scene, p->lo, p->hi);

@@ -63,11 +63,17 @@ cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, c
 
 cudaError_t launch_fast_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
                                 const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
-                                uint32_t refill) {
+                                uint32_t refill, int uniform_mode) {
   if (total == 0) return cudaSuccess;
   using rtk::ManyBatches;
   const ManyBatches src{table, entries, order};
-  if (s.layout == 0) return run(rtk::k_gi_fast<2, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+  if (s.layout == 0) {
+    if (uniform_mode == 0) return run(rtk::k_gi_fast<0, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+    if (uniform_mode == 1) return run(rtk::k_gi_fast<1, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+    return run(rtk::k_gi_fast<2, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+  }
+  if (uniform_mode == 0) return run(rtk::k_rs_fast<0, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+  if (uniform_mode == 1) return run(rtk::k_rs_fast<1, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
   return run(rtk::k_rs_fast<2, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
 }
 

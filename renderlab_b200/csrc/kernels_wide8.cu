@@ -73,15 +73,16 @@ cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, v
 
 cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
                                  const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
-                                 uint32_t refill) {
+                                 uint32_t refill, int uniform_mode) {
   if (total == 0) return cudaSuccess;
   rtk::W8View v;
   if (!view_of(s, v)) return cudaErrorInvalidValue;
   using rtk::ManyBatches;
   const ManyBatches src{table, entries, order};
-  if (s.layout == 0)
-    return run(rtk::k_wide8<0, 2, W8_BLOCK, false, ManyBatches>, s.words, v, src, counter, total, st, stream, nullptr, refill);
-  return run(rtk::k_wide8<1, 2, W8_BLOCK, false, ManyBatches>, s.words, v, src, counter, total, st, stream, nullptr, refill);
+#define RT_W8B(L, AM) run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches>, s.words, v, src, counter, total, st, stream, nullptr, refill)
+  if (s.layout == 0) return uniform_mode == 0 ? RT_W8B(0, 0) : (uniform_mode == 1 ? RT_W8B(0, 1) : RT_W8B(0, 2));
+  return uniform_mode == 0 ? RT_W8B(1, 0) : (uniform_mode == 1 ? RT_W8B(1, 1) : RT_W8B(1, 2));
+#undef RT_W8B
 }
 
 }  // namespace rtl

@@ -33,13 +33,15 @@ cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, c
 cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                          uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
 // Many batches in one persistent launch: `table` (device, `entries` records sorted by `first`)
-// covers `total` rays; `order` (optional) permutes the launch's ray space. Mode per entry.
+// covers `total` rays; `order` (optional) permutes the launch's ray space. Mode per entry;
+// `uniform_mode` 0 / 1 when every non-empty entry is closest / any hit (a kernel with the mode
+// fixed), -1 for a mix.
 cudaError_t launch_fast_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
                                 const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
-                                uint32_t refill);
+                                uint32_t refill, int uniform_mode);
 cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
                                  const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
-                                 uint32_t refill);
+                                 uint32_t refill, int uniform_mode);
 // WIDE8 with per-event device counters (rtk::W8Count order) accumulated into cnt[8].
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream);

@@ -3,8 +3,9 @@ traversal by timing candidate plans on the device.
 
 Parameters searched (each candidate is one rt_plan, timed as a whole, sort included):
 
-* kernel -- FAST (BVH4-Q8, bit-exact with the reference loop) or WIDE8 (8-wide compressed
-  nodes, watertight f32 test with f64 re-tests);
+* kernel -- PLAIN (one thread per ray, a launch per batch), FAST (persistent warps over the
+  BVH4-Q8, bit-exact with the reference loop like PLAIN) or WIDE8 (8-wide compressed nodes,
+  watertight f32 test with f64 re-tests);
 * wavefront width -- the refill threshold: how many lanes of a 32-wide warp must be idle before
   the warp takes more rays (1 keeps every lane busy; 32 hands out whole runs of 32 consecutive
   rays, which keeps a coherent batch's 8 x 4 tiles together);
@@ -23,7 +24,7 @@ import numpy as np
 
 from . import api as A
 
-KERNELS = ("fast", "wide8")
+KERNELS = ("plain", "fast", "wide8")
 REFILLS = (4, 8, 16, 32)
 ORDERS = ("none", "origin", "octant")
 
@@ -74,8 +75,10 @@ def candidates(kernels=KERNELS, refills=REFILLS, orders=ORDERS) -> list:
     """Every (kernel, refill, order), the usual winners first: unsorted before sorted, the middle
     and widest wavefronts before the rest."""
     pri = {8: 0, 32: 1, 16: 2, 4: 3}
-    return sorted(((k, r, o) for k in kernels for r in refills for o in orders),
-                  key=lambda c: (orders.index(c[2]) > 0, pri.get(c[1], 4), kernels.index(c[0])))
+    grid = [(k, r, o) for k in kernels for r in refills for o in orders if k != "plain"]
+    if "plain" in kernels:  # no ray queue and no sort: one candidate
+        grid.append(("plain", 0, orders[0]))
+    return sorted(grid, key=lambda c: (orders.index(c[2]) > 0, pri.get(c[1], 4), kernels.index(c[0])))
 
 
 def tune(engine: A.Engine, scene: A.Scene, batches, kernels=KERNELS, refills=REFILLS, orders=ORDERS,

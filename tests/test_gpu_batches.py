@@ -22,7 +22,7 @@ def _torch():
     return torch
 
 
-def _scene_and_batches(layout, seed=3):
+def _scene_and_batches(layout, seed=3, modes="mixed"):
     """One cube BLAS under a top level of 900 instances (every fifth casts no shadow), and 9
     batches of uneven sizes (one empty) alternating closest / any hit."""
     mesh, inst = S.cubes_instanced(30)
@@ -37,6 +37,8 @@ def _scene_and_batches(layout, seed=3):
     for k, n in enumerate(sizes):
         idx = rng.integers(0, len(pool), n)
         mode = A.CLOSEST if k % 2 == 0 else (A.ANY_CASTERS if k % 4 == 1 else A.ANY_SKY)
+        if modes != "mixed":  # every batch closest, or every batch any hit
+            mode = A.CLOSEST if modes == "closest" else (A.ANY_CASTERS if k % 2 else A.ANY_SKY)
         batches.append((np.ascontiguousarray(pool[idx]), mode))
     return words, batches
 
@@ -63,11 +65,12 @@ def _same(got, want, what):
         assert torch.equal(g, w), f"{what}: batch {k}: {(g != w).reshape(len(g), -1).any(1).sum().item()} rays differ"
 
 
+@pytest.mark.parametrize("modes", ["mixed", "closest", "any"])
 @pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
-@pytest.mark.parametrize("kernel", ["fast", "wide8"])
-def test_batches_equal_alone(engine, layout, kernel):
+@pytest.mark.parametrize("kernel", ["plain", "fast", "wide8"])
+def test_batches_equal_alone(engine, layout, kernel, modes):
     torch = _torch()
-    words, batches = _scene_and_batches(layout)
+    words, batches = _scene_and_batches(layout, modes=modes)
     scene = engine.upload(layout, words)
     try:
         if kernel == "wide8":
@@ -77,7 +80,7 @@ def test_batches_equal_alone(engine, layout, kernel):
         got = engine.trace_batches(scene, dev, kernel)
         torch.cuda.synchronize()
         _same(got, want, f"{kernel} one launch")
-        if kernel == "fast":  # and the oracle's, for the bit-exact kernel
+        if kernel != "wide8":  # and the oracle's, for the bit-exact kernels
             for (r, m), g in zip(batches, got):
                 if len(r) == 0:
                     continue
@@ -129,8 +132,6 @@ def test_batch_rejections(engine):
         dev = _device(batches[:2])
         with pytest.raises(A.RtError, match="UNSUPPORTED"):
             engine.trace_batches(scene, dev, "wide8")  # not prepared
-        with pytest.raises(A.RtError, match="UNSUPPORTED"):
-            engine.trace_batches(scene, dev, "plain")
         r = torch.zeros((8, 8), dtype=torch.float32, device="cuda")
         with pytest.raises(A.RtError, match="INVALID_ARG"):
             engine.trace_batches(scene, [(r.view(-1)[1:17].view(2, 8), A.CLOSEST)], "fast")  # 4-byte offset
@@ -153,7 +154,7 @@ def test_tuner_plan_matches_plain(engine):
         scene.prepare("wide8")
         dev = _device(batches)
         ch = T.tune(engine, scene, dev, refills=(8, 32), orders=("none", "octant"), reps=1)
-        assert {t.kernel for t in ch.trials} == {"fast", "wide8"} and len(ch.trials) == 8
+        assert {t.kernel for t in ch.trials} == {"plain", "fast", "wide8"} and len(ch.trials) == 9
         ch.plan.launch()
         torch.cuda.synchronize()
         plain = _alone(engine, scene, dev, "plain")
