@@ -12,6 +12,11 @@ Workloads (seeded synthetic scenes and rays; splitmix64, seed 0x5EED0000 + confi
   (4096 x 2048), 30 % GI hemisphere, 20 % shadow any-hit toward 16 point lights.
 * --config 4 batching: 64 BLAS (2k-500k triangles, log-uniform) under 10,000 randomly rotated,
   scaled and placed instances; 64 ray batches (1k-2M rays, log-uniform), closest / any hit.
+* --config 5 serving: 8 resident scenes (100k-8M triangles, BLAS + TLAS as config 4) under a
+  120 GB HBM budget; Poisson request arrivals at each --rates value; each request 4k-4M rays
+  (log-uniform) of shadow any-hit / GI closest / reflection closest (40/40/20) on a uniformly
+  chosen scene, from pinned host memory to pinned host memory through rt_server; beside it the
+  plain kernel serving the same arrivals one request at a time.
 
 Per step, the "plain" arm launches the plain kernel once per batch; the product arm replays the
 plans the autotuner chose (kernel, wavefront width, sort key; one CUDA graph per plan). Scenes
@@ -50,7 +55,9 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4])
+    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--rates", default="1000,2000,5000,10000,20000", help="--config 5: Poisson arrival rates (req/s)")
+    ap.add_argument("--requests", type=int, default=48, help="--config 5: requests per rate")
     ap.add_argument("--kernel", default="auto", help="auto: the autotuner's choice; or plain / fast / wide8")
     ap.add_argument("--refill", type=int, default=0, help="with --kernel fast/wide8: the wavefront width")
     ap.add_argument("--order", default="none", help="with --kernel fast/wide8: the sort key")
@@ -347,10 +354,38 @@ class HostScene:
         return self
 
 
+def reference_serving(args):
+    """Config 5 on the host cores: the oracle over a sample of every scene's three ray kinds."""
+    from renderlab_b200 import scenes as S
+    scenes = serving_scenes(args.small)
+    rng = S.Stream(S.seed_for(5) + 7)
+    threads = os.cpu_count() or 1
+    n, wall = 0, 0.0
+    for m in scenes:
+        words = oracle_pack(1, m.meshes, m.instances)
+        for kind, mode in (("shadow", 2), ("gi", 0), ("refl", 0)):
+            rays = serving_rays(kind, 256, 500.0, rng)
+            t0 = time.perf_counter()
+            oracle_trace(words, 1, rays, mode, threads=threads)
+            wall += time.perf_counter() - t0
+            n += len(rays)
+    value = n / wall / 1e6
+    return value, dict(value=value, unit=UNIT, cores=threads, kind="port",
+                       sample=f"{n:,} rays: 256 of each kind per scene, oracle rs_trace on {threads} threads, {wall:.2f} s")
+
+
 def run_reference(args):
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if int(os.environ.get("RANK", "0")) != 0:
         return  # rank 0 alone times the host-core reference
+    if args.config == 5:
+        value, cpu_line = reference_serving(args)
+        print(json.dumps(dict(metric=METRIC, value=value, unit=UNIT, impl="reference", n_gpus=world, steps=args.steps,
+                              warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
+                              data="synthetic", config=dict(workload="serving scenes (config 5), oracle sample", config=5),
+                              cpu_baseline=cpu_line, ms_per_step=None,
+                              e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0))), flush=True)
+        return
     holder = HostScene()
 
     def cpu_closest(engine, scene, rays, mode):
@@ -375,6 +410,131 @@ def run_reference(args):
                 ms_per_step=None, note="oracle restatement of the WGSL traversal loop on the host cores: the Rust/WGSL "
                                        "reference cannot run here (no rustc, no Vulkan/wgpu)")
     print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------- serving (config 5)
+
+def serving_scenes(small: bool):
+    """8 scenes, triangle counts log-uniform in [1e5, 8e6] (in [2.5e4, 2e6] with --small): 8 BLAS
+    each (log-uniform shares) under 512 instances placed as in config 4."""
+    from renderlab_b200 import scenes as S
+    s = S.Stream(S.seed_for(5))
+    lo, hi = (1e5, 8e6) if not small else (2.5e4, 2e6)
+    totals = np.round(np.exp(s.range(np.log(lo), np.log(hi), 8))).astype(np.int64)
+    out = []
+    for k, t in enumerate(totals):
+        ms = S.multi_blas(n_blas=8, n_instances=512, tri_lo=max(500.0, t / 16), tri_hi=max(1000.0, t / 4),
+                          config=5 + 16 * (k + 1))
+        out.append(ms)
+    return out
+
+
+def serving_rays(kind: str, n: int, half: float, stream):
+    from renderlab_b200 import scenes as S
+    o = stream.range(-half, half, n, 3)
+    if kind == "shadow":  # toward a random point of the box, stopping short of it
+        v = stream.range(-half, half, n, 3) - o
+        dist = np.maximum(np.linalg.norm(v, axis=1), 1e-3)
+        return S.pack_rays(o, v / dist[:, None], 0.0, dist * (1.0 - 1e-4))
+    return S.pack_rays(o, stream.unit_vectors(n), 0.0, 1e30)
+
+
+def run_serving(args):
+    import threading
+    import torch
+    from renderlab_b200 import api as A
+    from renderlab_b200 import scenes as S
+    engine = A.Engine(0)
+    kernel = "wide8" if args.kernel == "auto" else args.kernel
+    scenes = serving_scenes(args.small)
+    words = [engine_pack(A.LAYOUT_REFLECTION, m.meshes, m.instances) for m in scenes]
+    tris = [sum(x.triangles for x in m.meshes) for m in scenes]
+    budget = 120 << 30
+    srv = A.Server(engine, hbm_budget=budget, launch_rays=1 << 22, slots=4, kernel=kernel)
+    ids = [srv.add_scene(A.LAYOUT_REFLECTION, w) for w in words]
+    plain_scenes = [engine.upload(A.LAYOUT_REFLECTION, w) for w in words]
+    rng = S.Stream(S.seed_for(5) + 7)
+    lo, hi = (4e3, 4e6) if not args.small else (1e3, 1e6)
+    pools = {k: torch.from_numpy(serving_rays(k, int(hi), 500.0, rng)).pin_memory() for k in ("shadow", "gi", "refl")}
+    rates = [float(x) for x in args.rates.split(",")]
+    per_rate = []
+    total_rays, total_s = 0, 0.0
+    for rate in rates:
+        n_req = args.requests
+        gaps = -np.log(1.0 - rng.uniform(n_req)) / rate
+        arrive = np.cumsum(gaps)
+        sizes = np.round(np.exp(rng.range(np.log(lo), np.log(hi), n_req))).astype(np.int64)
+        u = rng.uniform(n_req)
+        kinds = np.where(u < 0.4, "shadow", np.where(u < 0.8, "gi", "refl"))
+        which = np.minimum((rng.uniform(n_req) * len(ids)).astype(np.int64), len(ids) - 1)
+        modes = [A.ANY_CASTERS if k == "shadow" else A.CLOSEST for k in kinds]
+        reqs = [(int(which[i]), modes[i], pools[kinds[i]][: int(sizes[i])]) for i in range(n_req)]
+        # every request its own slice of one pinned output buffer (overlapping requests share none)
+        words_of = [5 if m == A.CLOSEST else 1 for m in modes]
+        pool = torch.empty(int(sum(int(z) * w for z, w in zip(sizes, words_of))), dtype=torch.int32).pin_memory()
+        outs, at = [], 0
+        for z, w in zip(sizes, words_of):
+            outs.append(pool[at: at + int(z) * w].view(int(z), w) if w > 1 else pool[at: at + int(z)])
+            at += int(z) * w
+        srv.stats(reset=True)
+        tickets = [None] * n_req
+        t0 = time.perf_counter()
+
+        def producer():
+            for i, (sid, mode, rays) in enumerate(reqs):
+                delay = t0 + arrive[i] - time.perf_counter()
+                if delay > 0:
+                    time.sleep(delay)
+                tickets[i] = srv.submit(ids[sid], rays, mode, out=outs[i])
+
+        th = threading.Thread(target=producer)
+        th.start()
+        th.join()
+        for t in tickets:
+            srv.wait(t)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        rays = int(sizes.sum())
+        # the plain kernel, one request at a time, on the same arrivals
+        lat = []
+        t0 = time.perf_counter()
+        for i, (sid, mode, rays_i) in enumerate(reqs):
+            delay = t0 + arrive[i] - time.perf_counter()
+            if delay > 0:
+                time.sleep(delay)
+            engine.trace_host(plain_scenes[sid], rays_i, mode, "plain", out=outs[i])
+            lat.append((time.perf_counter() - t0 - arrive[i]) * 1e3)
+        wall_plain = time.perf_counter() - t0
+        per_rate.append(dict(rate=rate, requests=n_req, rays=rays, mrays=rays / wall / 1e6, p50_ms=st["p50_ms"],
+                             p99_ms=st["p99_ms"], max_ms=st["max_ms"], launches=st["launches"],
+                             offered_mrays=rays / float(arrive[-1]) / 1e6,
+                             plain=dict(mrays=rays / wall_plain / 1e6, p50_ms=float(np.percentile(lat, 50)),
+                                        p99_ms=float(np.percentile(lat, 99)), max_ms=float(np.max(lat)))))
+        total_rays += rays
+        total_s += wall
+    dev_bytes = srv.stats()["device_bytes"]
+    srv.close()
+    for sc in plain_scenes:
+        sc.release()
+    top = per_rate[-1]
+    line = dict(metric=METRIC, value=total_rays / total_s / 1e6, unit=UNIT, n_gpus=1, steps=len(rates) * args.requests,
+                warmup=0, ms_per_step=total_s / (len(rates) * args.requests) * 1e3, higher_is_better=True,
+                scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
+                config=dict(workload=f"serving: 8 scenes ({', '.join(f'{t:,}' for t in tris)} triangles; 8 BLAS + "
+                                     f"TLAS of 512 instances each) resident under a {budget >> 30} GB HBM budget "
+                                     f"({dev_bytes / 1e9:.1f} GB used); Poisson arrivals, {args.requests} requests a "
+                                     f"rate of {int(lo):,}-{int(hi):,} rays (shadow / GI / reflection 40/40/20)",
+                            config=5, kernel=kernel, launch_rays=1 << 22, slots=4),
+                latency_ms=dict(p50=top["p50_ms"], p99=top["p99_ms"], plain_p50=top["plain"]["p50_ms"],
+                                plain_p99=top["plain"]["p99_ms"]),
+                rates=per_rate,
+                e2e=dict(value=total_rays / total_s / 1e6, unit=UNIT, h2d_bytes_per_step=None, d2h_bytes_per_step=None,
+                         path="rt_server_submit / rt_server_wait, pinned host buffers; timed from each rate's first "
+                              "arrival to its last completion"),
+                note="a step is one request; value = rays served / wall time over all rates")
+    print(json.dumps(line), flush=True)
+    engine.close()
+
 
 
 def run_ours(args):
@@ -583,6 +743,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.config == 5:
+        run_serving(args)
     else:
         run_ours(args)
     if int(os.environ.get("WORLD_SIZE", "1")) > 1:

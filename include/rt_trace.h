@@ -201,6 +201,46 @@ rt_status rt_plan_launch(rt_plan* plan, void* stream);
 rt_status rt_plan_info(const rt_plan* plan, uint64_t* rays, uint64_t* device_bytes);
 rt_status rt_plan_destroy(rt_plan* plan);
 
+/* ---- Serving ---------------------------------------------------------------------------
+ * A request loop over several device-resident scenes: requests (host ray buffers of any size,
+ * any mode) are submitted from any thread at any time and their hits written back to the
+ * caller's host buffers. Scenes are admitted only while scenes plus launch slots fit
+ * hbm_budget (else RT_ERR_OOM). A worker thread fills each free launch slot (launch_rays rays
+ * of device buffers, its own stream) with chunks of pending requests of one scene in arrival
+ * order and traces it with one many-batch launch of `kernel`; requests that arrive while slots
+ * are busy join the next free slot, and the slots' copies and launches overlap on the device.
+ * Each ray's result equals that of the same ray traced alone with the same kernel. No
+ * counterpart in the reference (its passes trace inside the frame). Buffers of a request must
+ * stay valid until rt_server_wait returns for it; pinned host buffers keep the copies
+ * asynchronous. */
+typedef struct rt_server rt_server;
+typedef struct rt_server_desc {
+  uint64_t hbm_budget;  /* device bytes for scenes + launch slots */
+  uint32_t launch_rays; /* rays a launch slot holds (a request larger than this spans slots) */
+  uint32_t slots;       /* launch slots in flight at once (1-64) */
+  rt_kernel kernel;     /* RT_KERNEL_PLAIN, RT_KERNEL_FAST or RT_KERNEL_WIDE8 (scenes prepared on add) */
+} rt_server_desc;
+typedef struct rt_server_stats {
+  uint64_t requests;    /* finished since the last reset */
+  uint64_t rays;        /* traced since the last reset */
+  uint64_t launches;
+  double p50_ms, p99_ms, max_ms; /* request latency, submit to hits in host memory */
+  double wall_s;        /* since the last reset */
+  uint64_t device_bytes; /* resident scenes + launch slots */
+  uint64_t pending;     /* requests with rays not yet on the device */
+} rt_server_stats;
+rt_status rt_server_create(rt_ctx* ctx, const rt_server_desc* desc, rt_server** out);
+rt_status rt_server_add_scene(rt_server* srv, rt_layout layout, const uint32_t* words, size_t n_words, uint32_t* id);
+rt_status rt_server_remove_scene(rt_server* srv, uint32_t id); /* RT_ERR_BUSY while it has requests */
+rt_status rt_server_submit(rt_server* srv, uint32_t scene, rt_mode mode, const rt_ray* h_rays, uint32_t n,
+                           void* h_hits, uint64_t* ticket);
+/* Waits for a request (timeout_ms < 0: no limit); RT_ERR_TIMEOUT leaves it waitable again.
+ * Returns the request's status and forgets the ticket. */
+rt_status rt_server_wait(rt_server* srv, uint64_t ticket, int32_t timeout_ms);
+rt_status rt_server_get_stats(rt_server* srv, rt_server_stats* out, int reset);
+/* Finishes every submitted request, then frees the slots and releases the scenes. */
+rt_status rt_server_destroy(rt_server* srv);
+
 /* Host-buffer form: copies rays in and hits out through the context's pinned staging and
  * device buffers (grown on first use, or sized ahead by rt_ctx_reserve), pipelined in chunks
  * over two streams. Returns when the hits are in h_hits. */

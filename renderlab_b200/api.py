@@ -63,6 +63,17 @@ class RtPlanDesc(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("refill", ctypes.c_uint32), ("order", ctypes.c_int), ("graph", ctypes.c_uint32)]
 
 
+class RtServerDesc(ctypes.Structure):
+    _fields_ = [("hbm_budget", ctypes.c_uint64), ("launch_rays", ctypes.c_uint32), ("slots", ctypes.c_uint32),
+                ("kernel", ctypes.c_int)]
+
+
+class RtServerStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_uint64), ("rays", ctypes.c_uint64), ("launches", ctypes.c_uint64),
+                ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double), ("max_ms", ctypes.c_double),
+                ("wall_s", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("pending", ctypes.c_uint64)]
+
+
 class RtTuning(ctypes.Structure):
     _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
@@ -72,6 +83,8 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
+           "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
+           "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
            "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
 
@@ -115,6 +128,14 @@ def lib() -> ctypes.CDLL:
     L.rt_plan_launch.argtypes = [_vp, _vp]
     L.rt_plan_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.rt_plan_destroy.argtypes = [_vp]
+    L.rt_server_create.argtypes = [_vp, ctypes.POINTER(RtServerDesc), ctypes.POINTER(_vp)]
+    L.rt_server_add_scene.argtypes = [_vp, ctypes.c_int, _u32p, ctypes.c_size_t, _u32p]
+    L.rt_server_remove_scene.argtypes = [_vp, ctypes.c_uint32]
+    L.rt_server_submit.argtypes = [_vp, ctypes.c_uint32, ctypes.c_int, _vp, ctypes.c_uint32, _vp,
+                                   ctypes.POINTER(ctypes.c_uint64)]
+    L.rt_server_wait.argtypes = [_vp, ctypes.c_uint64, ctypes.c_int32]
+    L.rt_server_get_stats.argtypes = [_vp, ctypes.POINTER(RtServerStats), ctypes.c_int]
+    L.rt_server_destroy.argtypes = [_vp]
     L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
@@ -317,6 +338,69 @@ class Plan:
         if self.handle:
             lib().rt_plan_destroy(self.handle)
             self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Server:
+    """The serving loop (rt_server_*): submit host ray batches for resident scenes from any
+    thread, wait for their hits. Keeps each request's buffers alive until it is waited for."""
+
+    def __init__(self, engine: "Engine", hbm_budget: int, launch_rays: int = 1 << 22, slots: int = 4,
+                 kernel: str = "wide8"):
+        self.engine = engine
+        desc = RtServerDesc(int(hbm_budget), int(launch_rays), int(slots), KERNELS[kernel])
+        h = _vp()
+        engine._check(lib().rt_server_create(engine.ctx, ctypes.byref(desc), ctypes.byref(h)))
+        self.handle, self.kernel, self.layouts, self._held = h, kernel, {}, {}
+
+    def add_scene(self, layout: int, words) -> int:
+        w = np.ascontiguousarray(words, np.uint32)
+        sid = ctypes.c_uint32()
+        self.engine._check(lib().rt_server_add_scene(self.handle, layout, _np_ptr(w, _u32p), len(w), ctypes.byref(sid)))
+        self.layouts[sid.value] = layout
+        return sid.value
+
+    def remove_scene(self, sid: int):
+        self.engine._check(lib().rt_server_remove_scene(self.handle, sid))
+
+    def submit(self, sid: int, rays, mode: int = CLOSEST, out=None) -> int:
+        """rays: (n, 8) float32 host array (numpy, or a pinned torch CPU tensor). Returns a ticket."""
+        n = len(rays)
+        words = hit_words(self.layouts[sid], mode)
+        if out is None:
+            out = np.zeros((n, words) if words > 1 else (n,), np.uint32)
+        rp = rays.data_ptr() if hasattr(rays, "data_ptr") else rays.ctypes.data
+        hp = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+        t = ctypes.c_uint64()
+        self.engine._check(lib().rt_server_submit(self.handle, sid, mode, rp if n else None, n, hp if n else None,
+                                                  ctypes.byref(t)))
+        self._held[t.value] = (rays, out)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1):
+        """The request's hits (raises RtError TIMEOUT if it is still running after timeout_ms)."""
+        st = lib().rt_server_wait(self.handle, ticket, timeout_ms)
+        if st == 5:
+            raise RtError(st, "request still running")
+        rays, out = self._held.pop(ticket)
+        self.engine._check(st)
+        return out
+
+    def stats(self, reset: bool = False) -> dict:
+        s = RtServerStats()
+        self.engine._check(lib().rt_server_get_stats(self.handle, ctypes.byref(s), 1 if reset else 0))
+        return {f: (float(getattr(s, f)) if t is ctypes.c_double else int(getattr(s, f))) for f, t in RtServerStats._fields_}
+
+    def close(self):
+        if self.handle:
+            lib().rt_server_destroy(self.handle)
+            self.handle = None
+            self._held.clear()
 
     def __del__(self):
         try:
