@@ -64,6 +64,8 @@ def parse(argv=None):
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--small", action="store_true", help="a reduced workload (profiling captures)")
+    ap.add_argument("--precision", type=int, default=-1,
+                    help="rays checked against the FP64 oracle (default: 65,536 for --config 3, else 0)")
     return ap.parse_args(argv)
 
 
@@ -315,6 +317,52 @@ def cpu_baseline_leg(wl: Workload, target_s: float, threads=None):
                 sample=f"{n:,} rays ({100 * frac:.2f} % of each batch of the step, strided), oracle "
                        f"{'gi_traverse' if wl.layout == 0 else 'rs_trace'} (scalar f32 C++) on {threads} threads, "
                        f"{wall:.2f} s"), (counts, [len(r) for r in sample])
+
+
+def precision_report(wl: Workload, results: dict, n_sample: int) -> dict:
+    """Hit identity and t of each arm's results against the FP64 oracle on a strided sample of
+    every batch. A near tie is a differing closest hit whose t lies within 1e-6 relative of the
+    FP64 t; t errors are relative, over rays both hit."""
+    from oracle import oracle as O
+    frac = min(1.0, n_sample / max(1, wl.rays))
+    idx = [np.arange(0, len(b.rays), max(1, int(round(1 / frac)))) if len(b.rays) else np.zeros(0, np.int64)
+           for b in wl.batches]
+    ref = []
+    for b, ix in zip(wl.batches, idx):
+        ref.append(O.fp64_trace(wl.words, b.rays[ix], wl.layout, any_hit=b.mode != 0) if len(ix) else None)
+    out = {}
+    for arm, hits in results.items():
+        closest = any_rays = mism = ties = any_bad = 0
+        rel = []
+        for b, ix, r, h in zip(wl.batches, idx, ref, hits):
+            if r is None:
+                continue
+            got = h[ix]
+            r64, ident = r
+            ohit = r64[:, 0] > 0
+            if b.mode:
+                any_rays += len(ix)
+                any_bad += int(((got != 0) != ohit).sum())
+                continue
+            closest += len(ix)
+            cols = slice(1, 3) if wl.layout == 1 else slice(1, 5)
+            ocols = slice(2, 4) if wl.layout == 1 else slice(2, 6)
+            ghit = got[:, 1] != (0 if wl.layout == 1 else 0xFFFFFFFF)
+            t = got[:, 0].view(np.float32).astype(np.float64)
+            t64 = r64[:, 1]
+            both = ghit & ohit
+            same = (got[:, cols] == ident[:, ocols]).all(1)
+            m = (ghit != ohit) | (both & ~same)
+            tie = m & both & (np.abs(t - t64) <= 1e-6 * np.abs(t64))
+            mism += int(m.sum())
+            ties += int(tie.sum())
+            rel.append(np.abs(t[both] - t64[both]) / np.maximum(np.abs(t64[both]), 1e-30))
+        rel = np.concatenate(rel) if rel else np.zeros(0)
+        out[arm] = dict(closest_rays=closest, id_mismatch_rate=mism / max(1, closest), near_ties=ties,
+                        unexplained=mism - ties, t_rel_max=float(rel.max()) if len(rel) else 0.0,
+                        t_rel_mean=float(rel.mean()) if len(rel) else 0.0, any_rays=any_rays,
+                        any_mismatches=any_bad)
+    return out
 
 
 # ---------------------------------------------------------------- arms
@@ -711,6 +759,15 @@ def run_ours(args):
         return 1 + (1 if p.desc["order"] != "none" else 0)
 
     launches_per_step = sum(launches(g, p) for g, p in zip(wl.groups, plans))
+    n_prec = args.precision if args.precision >= 0 else (65_536 if args.config == 3 else 0)
+    precision = None
+    if n_prec:
+        prod = [None] * len(wl.batches)
+        for g, p in zip(wl.groups, plans):
+            for j, i in enumerate(g):
+                prod[i] = (p.hits[j] if p is not None else plain_hits[i]).cpu().numpy().view(np.uint32)
+        precision = precision_report(wl, {"product": prod, "plain": [h.cpu().numpy().view(np.uint32) for h in plain_hits]},
+                                     n_prec)
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
         higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
@@ -727,7 +784,7 @@ def run_ours(args):
         breakdown={("+".join(wl.batches[i].label for i in g) if len(g) <= 3 else f"{len(g)} batches"):
                    float(sum(len(wl.batches[i].rays) for i in g) / (prod_ms[:, k].mean() * 1e-3) / 1e6)
                    for k, g in enumerate(wl.groups)},
-        tuning=tables, wall_s=wall,
+        tuning=tables, wall_s=wall, precision_vs_fp64=precision,
         roofline=roof, cpu_baseline=cpu, clocks=clk, e2e=e2e, gpu_launches=launches_per_step * args.steps)
     if notes:
         line["notes"] = sorted(set(notes))
