@@ -321,8 +321,8 @@ def cpu_baseline_leg(wl: Workload, target_s: float, threads=None):
 
 def precision_report(wl: Workload, results: dict, n_sample: int) -> dict:
     """Hit identity and t of each arm's results against the FP64 oracle on a strided sample of
-    every batch. A near tie is a differing closest hit whose t lies within 1e-6 relative of the
-    FP64 t; t errors are relative, over rays both hit."""
+    every batch, per batch. A near tie is a differing closest hit whose t lies within 1e-6
+    relative of the FP64 t; t errors are relative, over rays whose hit identity matches."""
     from oracle import oracle as O
     frac = min(1.0, n_sample / max(1, wl.rays))
     idx = [np.arange(0, len(b.rays), max(1, int(round(1 / frac)))) if len(b.rays) else np.zeros(0, np.int64)
@@ -331,37 +331,32 @@ def precision_report(wl: Workload, results: dict, n_sample: int) -> dict:
     for b, ix in zip(wl.batches, idx):
         ref.append(O.fp64_trace(wl.words, b.rays[ix], wl.layout, any_hit=b.mode != 0) if len(ix) else None)
     out = {}
-    for arm, hits in results.items():
-        closest = any_rays = mism = ties = any_bad = 0
-        rel = []
-        for b, ix, r, h in zip(wl.batches, idx, ref, hits):
+    for arm, (hits, kernels) in results.items():
+        per = {}
+        for b, ix, r, h, kern in zip(wl.batches, idx, ref, hits, kernels):
             if r is None:
                 continue
             got = h[ix]
             r64, ident = r
             ohit = r64[:, 0] > 0
             if b.mode:
-                any_rays += len(ix)
-                any_bad += int(((got != 0) != ohit).sum())
+                per[b.label] = dict(kernel=kern, any_rays=len(ix), flag_mismatches=int(((got != 0) != ohit).sum()))
                 continue
-            closest += len(ix)
             cols = slice(1, 3) if wl.layout == 1 else slice(1, 5)
             ocols = slice(2, 4) if wl.layout == 1 else slice(2, 6)
             ghit = got[:, 1] != (0 if wl.layout == 1 else 0xFFFFFFFF)
             t = got[:, 0].view(np.float32).astype(np.float64)
             t64 = r64[:, 1]
             both = ghit & ohit
-            same = (got[:, cols] == ident[:, ocols]).all(1)
+            same = both & (got[:, cols] == ident[:, ocols]).all(1)
             m = (ghit != ohit) | (both & ~same)
             tie = m & both & (np.abs(t - t64) <= 1e-6 * np.abs(t64))
-            mism += int(m.sum())
-            ties += int(tie.sum())
-            rel.append(np.abs(t[both] - t64[both]) / np.maximum(np.abs(t64[both]), 1e-30))
-        rel = np.concatenate(rel) if rel else np.zeros(0)
-        out[arm] = dict(closest_rays=closest, id_mismatch_rate=mism / max(1, closest), near_ties=ties,
-                        unexplained=mism - ties, t_rel_max=float(rel.max()) if len(rel) else 0.0,
-                        t_rel_mean=float(rel.mean()) if len(rel) else 0.0, any_rays=any_rays,
-                        any_mismatches=any_bad)
+            rel = np.abs(t[same] - t64[same]) / np.maximum(np.abs(t64[same]), 1e-30)
+            per[b.label] = dict(kernel=kern, closest_rays=len(ix), id_mismatch_rate=float(m.sum()) / max(1, len(ix)),
+                                near_ties=int(tie.sum()), other_mismatches=int((m & ~tie).sum()),
+                                t_rel_max=float(rel.max()) if len(rel) else 0.0,
+                                t_rel_mean=float(rel.mean()) if len(rel) else 0.0)
+        out[arm] = per
     return out
 
 
@@ -766,8 +761,13 @@ def run_ours(args):
         for g, p in zip(wl.groups, plans):
             for j, i in enumerate(g):
                 prod[i] = (p.hits[j] if p is not None else plain_hits[i]).cpu().numpy().view(np.uint32)
-        precision = precision_report(wl, {"product": prod, "plain": [h.cpu().numpy().view(np.uint32) for h in plain_hits]},
-                                     n_prec)
+        kern = [None] * len(wl.batches)
+        for g, p in zip(wl.groups, plans):
+            for i in g:
+                kern[i] = p.desc["kernel"] if p is not None else "plain"
+        precision = precision_report(wl, {"product": (prod, kern),
+                                          "plain": ([h.cpu().numpy().view(np.uint32) for h in plain_hits],
+                                                    ["plain"] * len(wl.batches))}, n_prec)
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
         higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
