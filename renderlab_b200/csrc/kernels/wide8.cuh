@@ -120,8 +120,8 @@ struct W8Ray {
   uint32_t oct;
   // watertight shear rows: (Ax, Ay, Az) = M (v - o)
   F3 mx, my, mz;
-  float omax;   // |o|_inf
-  float tscale; // 8 u |1 / d_kz|: absolute error of t per unit of coordinate magnitude
+  float oerr;   // |o - o64|_inf: the f32 object-space origin against the f64 reference's
+  float tscale; // 8 u |1 / d_kz|: absolute error of t per unit of |v - o|
   bool valid;
 };
 
@@ -149,13 +149,15 @@ RT_DEV void w8_setup(W8Ray& R) {
   R.mx = row(kx, -sx);
   R.my = row(ky, -sy);
   R.mz = {kz == 0 ? sz : 0.0f, kz == 1 ? sz : 0.0f, kz == 2 ? sz : 0.0f};
-  R.omax = fmaxf(fmaxf(fabsf(R.o.x), fabsf(R.o.y)), fabsf(R.o.z));
   R.tscale = 8.0f * W8_U * fabsf(sz);
 }
 
-// Projected vertex (Ax, Ay, Az): one fixed chain of operations per vertex.
-RT_DEV F3 w8_project(const W8Ray& R, F3 v) {
+// Projected vertex (Ax, Ay, Az): one fixed chain of operations per vertex. `m` keeps the
+// largest |v - o| component seen; each component is one rounding of the exact difference, so
+// its error is relative to itself, not to |v| or |o|.
+RT_DEV F3 w8_project(const W8Ray& R, F3 v, float& m) {
   const F3 a = {__fsub_rn(v.x, R.o.x), __fsub_rn(v.y, R.o.y), __fsub_rn(v.z, R.o.z)};
+  m = fmaxf(m, fmaxf(fabsf(a.x), fmaxf(fabsf(a.y), fabsf(a.z))));
   return {__fmaf_rn(a.z, R.mx.z, __fmaf_rn(a.y, R.mx.y, __fmul_rn(a.x, R.mx.x))),
           __fmaf_rn(a.z, R.my.z, __fmaf_rn(a.y, R.my.y, __fmul_rn(a.x, R.my.x))),
           __fmaf_rn(a.z, R.mz.z, __fmaf_rn(a.y, R.mz.y, __fmul_rn(a.x, R.mz.x)))};
@@ -170,8 +172,9 @@ RT_DEV float w8_edge(float px, float py, float qx, float qy) {
 
 // Watertight test. Returns 0 miss, 1 hit, 2 uncertain (near an edge: the caller re-tests in
 // f64). On hit / uncertain, t, u, v hold the f32 estimate (t may be outside the range).
-RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v) {
-  const F3 A = w8_project(R, v0), B = w8_project(R, v1), C = w8_project(R, v2);
+RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v, float& dmax) {
+  dmax = 0.0f;
+  const F3 A = w8_project(R, v0, dmax), B = w8_project(R, v1, dmax), C = w8_project(R, v2, dmax);
   const float U = w8_edge(C.x, C.y, B.x, B.y);  // opposite v0
   const float V = w8_edge(A.x, A.y, C.x, C.y);  // opposite v1
   const float W = w8_edge(B.x, B.y, A.x, A.y);  // opposite v2
@@ -207,16 +210,14 @@ RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const 
   const F3 v0 = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
   const F3 v1 = {__uint_as_float(q0.w), __uint_as_float(q1.x), __uint_as_float(q1.y)};
   const F3 v2 = {__uint_as_float(q1.z), __uint_as_float(q1.w), __uint_as_float(q2.x)};
-  float t, u, v;
-  const int kind = w8_triangle(R, v0, v1, v2, t, u, v);
+  float t, u, v, dmax;
+  const int kind = w8_triangle(R, v0, v1, v2, t, u, v, dmax);
   if (kind == 0) return false;
   const uint32_t ident = q2.y, ref = q2.z;
   const float tmin = ray.tmin, tmax = ray.tmax;
-  // How far the f32 t may be from the f64 one: relative W8_TIE, or the absolute rounding of
-  // v - o at this magnitude (dominant for short hits far from the origin).
-  const float vmax = fmaxf(fmaxf(fmaxf(fabsf(v0.x), fabsf(v0.y)), fmaxf(fabsf(v0.z), fabsf(v1.x))),
-                           fmaxf(fmaxf(fabsf(v1.y), fabsf(v1.z)), fmaxf(fmaxf(fabsf(v2.x), fabsf(v2.y)), fabsf(v2.z))));
-  const float abs_err = R.tscale * (R.omax + vmax);
+  // How far the f32 t may be from the f64 one: relative W8_TIE, or the absolute part from the
+  // rounding of v - o (relative to |v - o|) and from the f32 origin's own error (oerr).
+  const float abs_err = R.tscale * (dmax + R.oerr);
   const float band = fmaxf(W8_TIE * fabsf(t), abs_err);
   // Clearly outside the range or clearly behind the current best: nothing to decide.
   if (kind == 1) {
@@ -373,6 +374,7 @@ template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i, unsigned long long* cnt) {
   const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;
   if (any_of<AM>(L) && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
+  w8_count<COUNT>(cnt, W8C_INSTANCE_TESTS);
   const W8Best& best = L.best;
   const float bound = best.hit ? best.t + 2.0f * best.band + 2.0f * W8_TIE * best.t : L.ray.tmax;
   if (!(slab_near(L.ray.o, L.world_inv, ld3(w, r + 12), ld3(w, r + 15), L.ray.tmin, bound) <= bound)) return;
@@ -382,6 +384,16 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   const float r10 = ldf(w, r + 4), r11 = ldf(w, r + 5), r12 = ldf(w, r + 6), r13 = ldf(w, r + 7);
   const float r20 = ldf(w, r + 8), r21 = ldf(w, r + 9), r22 = ldf(w, r + 10), r23 = ldf(w, r + 11);
   L.R.o = {dot4p(r00, r01, r02, r03, L.ray.o), dot4p(r10, r11, r12, r13, L.ray.o), dot4p(r20, r21, r22, r23, L.ray.o)};
+  {  // the origin of the f64 reference (ray64's arithmetic), to bound the f32 origin's error
+    const double ox = L.ray.o.x, oy = L.ray.o.y, oz = L.ray.o.z;
+    auto o64 = [&](float a, float b, float c, float d) {
+      return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, ox), __dmul_rn(b, oy)), __dmul_rn(c, oz)), (double)d);
+    };
+    const double ex = fabs(o64(r00, r01, r02, r03) - (double)L.R.o.x), ey = fabs(o64(r10, r11, r12, r13) - (double)L.R.o.y),
+                 ez = fabs(o64(r20, r21, r22, r23) - (double)L.R.o.z);
+    const double e = fmax(fmax(ex, ey), ez);
+    L.R.oerr = e > 0.0 ? __double2float_ru(e) : 0.0f;
+  }
   L.R.d = {dot3({r00, r01, r02}, L.ray.d), dot3({r10, r11, r12}, L.ray.d), dot3({r20, r21, r22}, L.ray.d)};
   w8_setup(L.R);
   if (!L.R.valid) return;
