@@ -207,6 +207,7 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
     for (int a = 0; a < 3; ++a) {
       p[a] = nb.lo[a];
       ex[a] = scale_exponent((double)nb.hi[a] - (double)p[a]);
+      out.max_exponent = std::max(out.max_exponent, ex[a]);
     }
     uint32_t imask = 0, child_base = (uint32_t)(out.nodes.size() / W8_NODE_WORDS),
              tri_base = (uint32_t)(out.tris.size() / W8_TRI_WORDS);
@@ -355,6 +356,10 @@ bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8
   std::vector<uint32_t> node_base(nb), tri_base(nb);
   size_t nn = 0, ntri = 0;
   for (size_t b = 0; b < nb; ++b) {
+    if (built[b].max_exponent > W8_MAX_EXPONENT) {
+      err = "a BLAS extends beyond 255 * 2^13 units on an axis: its 8-wide nodes cannot be decoded exactly";
+      return false;
+    }
     node_base[b] = (uint32_t)nn;
     tri_base[b] = (uint32_t)ntri;
     nn += built[b].nodes.size() / W8_NODE_WORDS;

@@ -3,7 +3,7 @@
 //
 // Node, 80 bytes (20 words, five 16-byte loads):
 //   0-2   p: float origin of the child boxes
-//   3     exponent bytes ex | ey << 8 | ez << 16 (scale 2^(e-127)), inner-child mask << 24
+//   3     exponent bytes ex | ey << 8 | ez << 16 (scale 2^(e-127), e - 127 <= 13), inner-child mask << 24
 //   4     index of the first inner child node (inner children are contiguous, in slot order)
 //   5     index of the first triangle (leaf children's triangles are contiguous, in slot order)
 //   6-7   meta byte per slot: leaf (count << 5 | offset), 0 for an inner or empty slot
@@ -28,10 +28,14 @@ namespace rtb {
 constexpr uint32_t W8_NODE_WORDS = 20;
 constexpr uint32_t W8_TRI_WORDS = 12;
 constexpr uint32_t W8_MAX_LEAF = 3;
+// Largest node scale exponent: the kernel multiplies 2^(e+15) by 1/d, which reaches 1e30, so
+// e <= 13 keeps the product finite (a BLAS at most 255 * 2^13 = 2,088,960 units wide).
+constexpr int W8_MAX_EXPONENT = 13;
 
 struct Wide8Blas {
   std::vector<uint32_t> nodes;  // root is node 0
   std::vector<uint32_t> tris;
+  int max_exponent = -126;      // the largest scale exponent of its nodes
 };
 
 // The whole derived scene: per distinct BLAS of the packed words, its nodes and triangles, and

@@ -4,9 +4,9 @@
 // * BLAS: 80-byte nodes; a ray's direction-sign octant o orders the children (slot k ^ o is
 //   visited k-th); inner hits form a node group (first child, pending bits, inner mask) that is
 //   pushed whole, so the stack holds one entry per level.
-// * Child boxes: t = fma(q, 2^e / d, (p - o) / d) per plane, widened by a per-node bound on its
-//   rounding error so that no box a ray meets is ever culled (the boxes themselves enclose their
-//   triangles exactly).
+// * Child boxes: t = fma(1 + q 2^-15, 2^(e+15) / d, (p - o) / d - 2^(e+15) / d) per plane (one
+//   byte permute and one fma), widened by a per-node bound on its rounding error so that no box a
+//   ray meets is ever culled (the boxes themselves enclose their triangles exactly).
 // * Triangles: the watertight test of Woop, Benthin and Wald (2013) through a per-instance
 //   shear matrix; an edge function that rounds to zero is recomputed in double. Shared vertices
 //   transform identically, so a ray never slips between two triangles.
@@ -262,8 +262,9 @@ RT_DEV uint32_t oct_permute(uint32_t m, uint32_t o) {
   return m;
 }
 
-RT_DEV float q_f(uint32_t word, uint32_t byte) {
-  return __fsub_rn(__uint_as_float(__byte_perm(word, 0x4B000000u, byte | 0x7540u)), 8388608.0f);
+// Byte `byte` of `word` as 1 + q * 2^-15, exactly: the byte lands in mantissa bits 8-15 of 1.0f.
+RT_DEV float q15(uint32_t word, uint32_t byte) {
+  return __uint_as_float(__byte_perm(word, 0x3F800000u, 0x7604u | (byte << 4)));
 }
 
 // The per-lane traversal state of the persistent WIDE8 kernel.
@@ -291,19 +292,23 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const uint4* np = V.nodes + 5 * (size_t)L.node;
   const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
   const float px = __uint_as_float(a0.x), py = __uint_as_float(a0.y), pz = __uint_as_float(a0.z);
-  const float Ax = __fmul_rn(__uint_as_float((a0.w & 0xffu) << 23), R.inv.x);
-  const float Ay = __fmul_rn(__uint_as_float(((a0.w >> 8) & 0xffu) << 23), R.inv.y);
-  const float Az = __fmul_rn(__uint_as_float(((a0.w >> 16) & 0xffu) << 23), R.inv.z);
+  // A' = 2^(e+15) / d and C = (p - o) / d - A' per axis, so that a plane's t = q 2^e / d + (p - o) / d
+  // is one fma of the decoded 1 + q 2^-15: fma(Q, A', C). The same rounded A' enters both terms,
+  // so its rounding cancels; exponents stay <= 13 (the builder's bound), so A' never overflows.
+  const float Ax = __fmul_rn(__uint_as_float(((a0.w & 0xffu) + 15u) << 23), R.inv.x);
+  const float Ay = __fmul_rn(__uint_as_float((((a0.w >> 8) & 0xffu) + 15u) << 23), R.inv.y);
+  const float Az = __fmul_rn(__uint_as_float((((a0.w >> 16) & 0xffu) + 15u) << 23), R.inv.z);
   const float Bx = __fmul_rn(__fsub_rn(px, R.o.x), R.inv.x), By = __fmul_rn(__fsub_rn(py, R.o.y), R.inv.y),
               Bz = __fmul_rn(__fsub_rn(pz, R.o.z), R.inv.z);
-  // Per axis, |error of a plane's t| <= u (255 |A| + 3 |B|) + u |t| (the rounding of 1/d, of
-  // p - o, of (p - o) / d and of the fma). The absolute part, doubled and with |B| taken four
-  // times to cover rounding B -/+ E itself, moves the near planes down and the far planes up;
-  // the relative part is applied to the entry / exit after the max / min.
-  const float Ex = 2.0f * W8_U * fmaf(255.0f, fabsf(Ax), 4.0f * fabsf(Bx));
-  const float Ey = 2.0f * W8_U * fmaf(255.0f, fabsf(Ay), 4.0f * fabsf(By));
-  const float Ez = 2.0f * W8_U * fmaf(255.0f, fabsf(Az), 4.0f * fabsf(Bz));
-  const float Bnx = Bx - Ex, Bfx = Bx + Ex, Bny = By - Ey, Bfy = By + Ey, Bnz = Bz - Ez, Bfz = Bz + Ez;
+  // Per axis, |error of a plane's t| <= u (2 * 255 * 2^-15 |A'| + 3 |B|) (the rounding of 1/d,
+  // of 2^e / d, of p - o and of (p - o) / d) + 2 u (|B| + |A'|) (the rounding of B - A' and of
+  // C -/+ E) + u |t| (the fma). The absolute part, doubled, moves the near planes down and the far
+  // planes up; the relative part is applied to the entry / exit after the max / min.
+  const float Ex = 2.0f * W8_U * fmaf(2.1f, fabsf(Ax), 6.0f * fabsf(Bx));
+  const float Ey = 2.0f * W8_U * fmaf(2.1f, fabsf(Ay), 6.0f * fabsf(By));
+  const float Ez = 2.0f * W8_U * fmaf(2.1f, fabsf(Az), 6.0f * fabsf(Bz));
+  const float Cx = __fsub_rn(Bx, Ax), Cy = __fsub_rn(By, Ay), Cz = __fsub_rn(Bz, Az);
+  const float Bnx = Cx - Ex, Bfx = Cx + Ex, Bny = Cy - Ey, Bfy = Cy + Ey, Bnz = Cz - Ez, Bfz = Cz + Ez;
   const uint32_t imask = a0.w >> 24;
   const uint32_t child_base = a1.x, tri_base = a1.y, meta_lo = a1.z, meta_hi = a1.w;
   // near / far planes per axis by the direction's sign
@@ -320,9 +325,9 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     const uint32_t b = s & 3;
-    const float tnx = fmaf(q_f(s < 4 ? nx0 : nx1, b), Ax, Bnx), tfx = fmaf(q_f(s < 4 ? fx0 : fx1, b), Ax, Bfx);
-    const float tny = fmaf(q_f(s < 4 ? ny0 : ny1, b), Ay, Bny), tfy = fmaf(q_f(s < 4 ? fy0 : fy1, b), Ay, Bfy);
-    const float tnz = fmaf(q_f(s < 4 ? nz0 : nz1, b), Az, Bnz), tfz = fmaf(q_f(s < 4 ? fz0 : fz1, b), Az, Bfz);
+    const float tnx = fmaf(q15(s < 4 ? nx0 : nx1, b), Ax, Bnx), tfx = fmaf(q15(s < 4 ? fx0 : fx1, b), Ax, Bfx);
+    const float tny = fmaf(q15(s < 4 ? ny0 : ny1, b), Ay, Bny), tfy = fmaf(q15(s < 4 ? fy0 : fy1, b), Ay, Bfy);
+    const float tnz = fmaf(q15(s < 4 ? nz0 : nz1, b), Az, Bnz), tfz = fmaf(q15(s < 4 ? fz0 : fz1, b), Az, Bfz);
     float tn = fmaxf(fmaxf(tnx, tny), tnz), tf = fminf(fminf(tfx, tfy), tfz);
     tn = fmaf(-2.0f * W8_U, fabsf(tn), tn);
     tf = fmaf(2.0f * W8_U, fabsf(tf), tf);

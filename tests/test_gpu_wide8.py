@@ -131,3 +131,20 @@ def test_wide8_grid_edges_are_watertight(engine):
         got = traced(engine, layout, w, rays, A.CLOSEST)
         hit = got[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)
         assert hit.all(), f"{(~hit).sum()} rays slipped through the grid"
+
+
+def test_wide8_refuses_blas_beyond_its_decode_range(engine):
+    """An 8-wide node decodes its planes as 2^(e+15) / d; exponents above 13 (a BLAS wider than
+    255 * 2^13 units) could overflow, so preparing such a scene is refused, and FAST still runs."""
+    p = np.array([[0, 0, 0], [3.0e6, 0, 0], [0, 1, 0]], np.float32)
+    i = np.array([0, 1, 2], np.uint32)
+    w = product_words(A.LAYOUT_REFLECTION, [S.Mesh(p, i)], S.identity_instances(1))
+    scene = engine.upload(A.LAYOUT_REFLECTION, w)
+    try:
+        with pytest.raises(A.RtError, match="LAYOUT"):
+            scene.prepare("wide8")
+        rays = np.array([[1.0, 0.25, -1.0, 0.0, 0.0, 0.0, 1.0, 10.0]], np.float32)
+        got = gpu_trace(engine, scene, rays, A.CLOSEST, "fast")
+        assert got[0, 1] != 0
+    finally:
+        scene.release()
