@@ -56,7 +56,9 @@ typedef enum rt_mode {
 typedef enum rt_kernel {
   RT_KERNEL_PLAIN = 0,
   RT_KERNEL_FAST = 1,
-  RT_KERNEL_WIDE8 = 2
+  RT_KERNEL_WIDE8 = 2,
+  RT_KERNEL_WIDE8_PACKET = 3 /* WIDE8 walked by warp-wide packets of 32 consecutive rays, for coherent
+                                batches over flat instance lists (no top level); WIDE8's results */
 } rt_kernel;
 
 /* One ray, 32 bytes: origin, tmin, direction (need not be unit length), tmax. */

@@ -26,7 +26,7 @@ LIB_PATH = Path(__file__).resolve().parent / "_lib" / "librt_trace.so"
 
 LAYOUT_GI, LAYOUT_REFLECTION = 0, 1
 CLOSEST, ANY_SKY, ANY_CASTERS = 0, 1, 2
-KERNELS = {"plain": 0, "fast": 1, "wide8": 2}
+KERNELS = {"plain": 0, "fast": 1, "wide8": 2, "wide8p": 3}
 ORDERS = {"none": 0, "origin": 1, "octant": 2, "direction": 3}
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "LAYOUT", 3: "OOM", 4: "STACK_OVERFLOW", 5: "TIMEOUT",
           6: "CUDA", 7: "BUSY", 8: "UNSUPPORTED"}

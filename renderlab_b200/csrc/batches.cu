@@ -19,9 +19,12 @@ constexpr uint64_t MAX_LAUNCH_RAYS = 1ull << 31;  // the ray counter's headroom 
 rt_status make_table(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const rt_batch* b, uint32_t n,
                      rtk::BatchEntry* table, uint64_t& total, int& uniform) {
   if (!scene) return fail(ctx, RT_ERR_INVALID_ARG, "null scene");
-  if (kernel != RT_KERNEL_PLAIN && kernel != RT_KERNEL_FAST && kernel != RT_KERNEL_WIDE8)
+  const bool wide = kernel == RT_KERNEL_WIDE8 || kernel == RT_KERNEL_WIDE8_PACKET;
+  if (kernel != RT_KERNEL_PLAIN && kernel != RT_KERNEL_FAST && !wide)
     return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
-  if (kernel == RT_KERNEL_WIDE8 && !scene->d_wide8)
+  if (kernel == RT_KERNEL_WIDE8_PACKET && scene->info.top != 0)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the packet walk takes flat instance lists only");
+  if (wide && !scene->d_wide8)
     return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
   if (n && !b) return fail(ctx, RT_ERR_INVALID_ARG, "null batch array");
   if (n > RT_MAX_BATCHES) return fail(ctx, RT_ERR_INVALID_ARG, "%u batches (at most %u)", n, RT_MAX_BATCHES);
@@ -71,6 +74,8 @@ cudaError_t enqueue(const rt_scene* scene, rt_kernel kernel, const rtk::BatchEnt
   const rtl::SceneView v = view_of(scene);
   if (kernel == RT_KERNEL_WIDE8)
     return rtl::launch_wide8_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform);
+  if (kernel == RT_KERNEL_WIDE8_PACKET)
+    return rtl::launch_wide8_packet_batches(v, d_table, entries, total, order, counter, st, s, uniform);
   return rtl::launch_fast_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform);
 }
 
@@ -117,7 +122,7 @@ rt_status rt_trace_batches(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel,
   }
   RT_CUDA(ctx, cudaMemcpyAsync(d, h, sizeof(rtk::BatchEntry) * n_batches, cudaMemcpyHostToDevice, s));
   RT_CUDA(ctx, cudaEventRecord(ctx->table_done[slot], s));
-  const uint32_t refill = kernel == RT_KERNEL_WIDE8 ? ctx->tuning.wide8_refill : ctx->tuning.fast_refill;
+  const uint32_t refill = kernel == RT_KERNEL_FAST ? ctx->tuning.fast_refill : ctx->tuning.wide8_refill;
   cudaError_t e = enqueue(scene, kernel, d, n_batches, (uint32_t)total, nullptr,
                           ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, s, refill, uniform);
   if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "many-batch launch: %s", cudaGetErrorString(e));
@@ -193,7 +198,7 @@ rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_b
   p->uniform = uniform;
   p->h_table = table;
   p->refill = desc->refill ? desc->refill
-                           : (desc->kernel == RT_KERNEL_WIDE8 ? ctx->tuning.wide8_refill : ctx->tuning.fast_refill);
+                           : (desc->kernel == RT_KERNEL_FAST ? ctx->tuning.fast_refill : ctx->tuning.wide8_refill);
   world_box(scene, p->lo, p->hi);
   auto oom = [&](const char* what, size_t bytes) {
     cudaGetLastError();

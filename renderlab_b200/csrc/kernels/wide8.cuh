@@ -282,15 +282,10 @@ struct W8Lane {
   uint32_t sp;
 };
 
-// One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
-// Returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, int AM, bool COUNT>
-RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st,
-                    unsigned long long* cnt) {
-  w8_count<COUNT>(cnt, W8C_NODES);
-  const W8Ray& R = L.R;
-  const uint4* np = V.nodes + 5 * (size_t)L.node;
-  const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
+// The eight child-box tests of one node for one ray: bit s is set when slot s's box meets
+// [tmin, lim] (conservatively: no box the ray meets is missed).
+RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, const uint4& a3, const uint4& a4, float tmin,
+                            float lim) {
   const float px = __uint_as_float(a0.x), py = __uint_as_float(a0.y), pz = __uint_as_float(a0.z);
   // A' = 2^(e+15) / d and C = (p - o) / d - A' per axis, so that a plane's t = q 2^e / d + (p - o) / d
   // is one fma of the decoded 1 + q 2^-15: fma(Q, A', C). The same rounded A' enters both terms,
@@ -309,8 +304,6 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const float Ez = 2.0f * W8_U * fmaf(2.1f, fabsf(Az), 6.0f * fabsf(Bz));
   const float Cx = __fsub_rn(Bx, Ax), Cy = __fsub_rn(By, Ay), Cz = __fsub_rn(Bz, Az);
   const float Bnx = Cx - Ex, Bfx = Cx + Ex, Bny = Cy - Ey, Bfy = Cy + Ey, Bnz = Cz - Ez, Bfz = Cz + Ez;
-  const uint32_t imask = a0.w >> 24;
-  const uint32_t child_base = a1.x, tri_base = a1.y, meta_lo = a1.z, meta_hi = a1.w;
   // near / far planes per axis by the direction's sign
   const uint32_t nx0 = R.oct & 1u ? a3.z : a2.x, nx1 = R.oct & 1u ? a3.w : a2.y;
   const uint32_t fx0 = R.oct & 1u ? a2.x : a3.z, fx1 = R.oct & 1u ? a2.y : a3.w;
@@ -318,9 +311,6 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const uint32_t fy0 = R.oct & 2u ? a2.z : a4.x, fy1 = R.oct & 2u ? a2.w : a4.y;
   const uint32_t nz0 = R.oct & 4u ? a4.z : a3.x, nz1 = R.oct & 4u ? a4.w : a3.y;
   const uint32_t fz0 = R.oct & 4u ? a3.x : a4.z, fz1 = R.oct & 4u ? a3.y : a4.w;
-  const W8Best& best = L.best;
-  const float lim = best.hit ? best.t + 2.0f * best.band + W8_TIE * best.t : L.ray.tmax;
-  const float tmin = L.ray.tmin;
   uint32_t hits = 0;
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
@@ -333,12 +323,31 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
     tf = fmaf(2.0f * W8_U, fabsf(tf), tf);
     if (fmaxf(tn, tmin) <= fminf(tf, lim)) hits |= 1u << s;
   }
-  // A slot is a leaf when its meta byte has a count; empty slots have neither.
-  const uint32_t leafmask = ((meta_lo & 0xe0u) ? 1u : 0u) | ((meta_lo & 0xe000u) ? 2u : 0u) |
-                            ((meta_lo & 0xe00000u) ? 4u : 0u) | ((meta_lo & 0xe0000000u) ? 8u : 0u) |
-                            ((meta_hi & 0xe0u) ? 16u : 0u) | ((meta_hi & 0xe000u) ? 32u : 0u) |
-                            ((meta_hi & 0xe00000u) ? 64u : 0u) | ((meta_hi & 0xe0000000u) ? 128u : 0u);
-  uint32_t leaf_hits = hits & leafmask;
+  return hits;
+}
+
+// A slot is a leaf when its meta byte has a count; empty slots have neither.
+RT_DEV uint32_t w8_leafmask(uint32_t meta_lo, uint32_t meta_hi) {
+  return ((meta_lo & 0xe0u) ? 1u : 0u) | ((meta_lo & 0xe000u) ? 2u : 0u) | ((meta_lo & 0xe00000u) ? 4u : 0u) |
+         ((meta_lo & 0xe0000000u) ? 8u : 0u) | ((meta_hi & 0xe0u) ? 16u : 0u) | ((meta_hi & 0xe000u) ? 32u : 0u) |
+         ((meta_hi & 0xe00000u) ? 64u : 0u) | ((meta_hi & 0xe0000000u) ? 128u : 0u);
+}
+
+// One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
+// Returns true when an any-hit query is satisfied.
+template <uint32_t LAYOUT, int AM, bool COUNT>
+RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st,
+                    unsigned long long* cnt) {
+  w8_count<COUNT>(cnt, W8C_NODES);
+  const W8Ray& R = L.R;
+  const uint4* np = V.nodes + 5 * (size_t)L.node;
+  const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
+  const uint32_t imask = a0.w >> 24;
+  const uint32_t child_base = a1.x, tri_base = a1.y, meta_lo = a1.z, meta_hi = a1.w;
+  const W8Best& best = L.best;
+  const float lim = best.hit ? best.t + 2.0f * best.band + W8_TIE * best.t : L.ray.tmax;
+  const uint32_t hits = w8_box_hits(R, a0, a2, a3, a4, L.ray.tmin, lim);
+  uint32_t leaf_hits = hits & w8_leafmask(meta_lo, meta_hi);
   while (leaf_hits) {
     const uint32_t s = __ffs(leaf_hits) - 1;
     leaf_hits &= leaf_hits - 1;
@@ -536,6 +545,98 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__
       w8_count<COUNT>(cnt, W8C_TOP_NODES);
       top_step(w, top_base + (size_t)item * 32, L.ray, L.world_inv, bound, tstack, L.tsp, st);
     }
+  }
+}
+
+// Packet walk, for coherent batches over flat instance lists: a warp takes 32 consecutive rays and
+// walks ONE 8-wide traversal for all of them. A node's child is visited when any lane's ray meets
+// its box, in the first entering lane's octant order, so every lane reads the same node (one
+// broadcast load) and no lane diverges on the walk; the traversal stack is the warp's, in shared
+// memory. Each lane still tests its own ray against every visited node's boxes (its own hits and
+// closest-hit bound) and against the triangles of the leaves its ray meets. WIDE8's results do not
+// depend on the visit order (conservative boxes, ties resolved in f64 on (t, instance,
+// triangle)), so each ray gets the hit the per-ray walk finds.
+template <uint32_t LAYOUT, int AM, int BLOCK, class Src>
+__global__ void __launch_bounds__(BLOCK, 4) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
+                                                           unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
+  __shared__ uint2 warp_stack[BLOCK / 32][W8_STACK];
+  uint2* stack = warp_stack[threadIdx.x >> 5];
+  const int lane = threadIdx.x & 31;
+  const uint32_t count = ld(w, 0);
+  for (;;) {
+    uint32_t base = 0;
+    if (lane == 0) base = atomicAdd(counter, 32u);
+    base = __shfl_sync(0xffffffffu, base, 0);
+    if (base >= n) break;
+    const uint32_t id = base + lane;
+    W8Lane L;
+    L.phase = 0;
+    bool live = id < n;  // the lane's ray still wants hits
+    if (live) {
+      L.ray = fetch(src, id, L);
+      L.world_inv = safe_inverse(L.ray.d);
+      W8Best& b = L.best;
+      b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.abs_err = 0.0f, b.t64 = 0.0;
+      b.inst = EMPTY, b.tri = 0, b.ident = 0, b.u = b.v = 0.0f;
+    }
+    for (uint32_t i = 0; i < count && __any_sync(0xffffffffu, live); ++i) {
+      L.phase = 0;
+      if (live) w8_enter<LAYOUT, AM, false>(w, V, L, i, nullptr);
+      bool in = L.phase == 2;
+      const unsigned entering = __ballot_sync(0xffffffffu, in);
+      if (!entering) continue;
+      const uint32_t oct = __shfl_sync(0xffffffffu, L.R.oct, __ffs(entering) - 1);
+      uint32_t node = __ldg(V.inst + 2 * (size_t)i), g_base = 0, g_bits = 0, g_imask = 0, sp = 0;
+      for (;;) {
+        if (node == EMPTY) {  // the warp's next node (uniform)
+          while (g_bits == 0 && sp > 0) {
+            const uint2 e = stack[--sp];
+            g_base = e.x, g_bits = e.y & 0xffu, g_imask = e.y >> 8;
+          }
+          if (g_bits == 0) break;
+          const uint32_t slot = (__ffs(g_bits) - 1) ^ oct;
+          g_bits &= g_bits - 1;
+          node = g_base + __popc(g_imask & ((1u << slot) - 1u));
+        }
+        const uint4* np = V.nodes + 5 * (size_t)node;
+        const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
+        const uint32_t imask = a0.w >> 24, child_base = a1.x, tri_base = a1.y, meta_lo = a1.z, meta_hi = a1.w;
+        uint32_t hits = 0;
+        if (in) {
+          const W8Best& best = L.best;
+          const float lim = best.hit ? best.t + 2.0f * best.band + W8_TIE * best.t : L.ray.tmax;
+          hits = w8_box_hits(L.R, a0, a2, a3, a4, L.ray.tmin, lim);
+        }
+        // leaves: every lane whose ray meets one tests its triangles
+        for (uint32_t lh = __reduce_or_sync(0xffffffffu, hits & w8_leafmask(meta_lo, meta_hi)); lh; lh &= lh - 1) {
+          const uint32_t s = __ffs(lh) - 1;
+          if (!in || !(hits >> s & 1u)) continue;
+          const uint32_t m = ((s < 4 ? meta_lo : meta_hi) >> (8 * (s & 3))) & 0xffu;
+          const uint32_t first = tri_base + (m & 31u), cnt = m >> 5;
+          for (uint32_t k = 0; k < cnt; ++k)
+            if (w8_candidate<LAYOUT, AM, false>(w, V, L.R, L.ray, L.inst, first + k, L.best, nullptr, L.any)) {
+              in = false, live = false;  // an any-hit ray is blocked
+              break;
+            }
+        }
+        const uint32_t inner = oct_permute(__reduce_or_sync(0xffffffffu, hits & imask), oct);
+        node = EMPTY;
+        if (!__any_sync(0xffffffffu, in)) break;
+        if (inner) {
+          if (g_bits) {
+            if (sp < W8_STACK) {
+              if (lane == 0) stack[sp] = make_uint2(g_base, g_bits | g_imask << 8);
+              __syncwarp();
+              ++sp;
+            } else if (lane == 0) {
+              atomicAdd(&st->stack_drops, 1ull);
+            }
+          }
+          g_base = child_base, g_bits = inner, g_imask = imask;
+        }
+      }
+    }
+    if (id < n) w8_finish<LAYOUT, AM, false>(w, V, L, out_of(src, L.entry), nullptr);
   }
 }
 

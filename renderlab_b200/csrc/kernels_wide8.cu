@@ -85,4 +85,47 @@ cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* tabl
 #undef RT_W8B
 }
 
+namespace {
+template <class K, class Src>
+cudaError_t run_packet(K kernel, const uint32_t* words, const rtk::W8View& v, const Src& src, unsigned int* counter,
+                       uint32_t n, rtk::DevStatus* st, cudaStream_t stream) {
+  uint32_t full = 0;
+  cudaError_t e = resident(kernel, full);
+  if (e != cudaSuccess) return e;
+  const uint32_t need = (n + W8_BLOCK - 1) / W8_BLOCK;
+  if ((e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), stream)) != cudaSuccess) return e;
+  kernel<<<need < full ? need : full, W8_BLOCK, 0, stream>>>(words, v, src, counter, n, st);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_wide8_packet(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
+                                uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  rtk::W8View v;
+  if (!view_of(s, v) || s.top != 0) return cudaErrorInvalidValue;
+  using rtk::OneBatch;
+  const OneBatch src{rays, order, hits};
+  if (s.layout == 0) {
+    if (mode == 0) return run_packet(rtk::k_wide8_packet<0, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+    return run_packet(rtk::k_wide8_packet<0, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+  }
+  if (mode == 0) return run_packet(rtk::k_wide8_packet<1, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+  return run_packet(rtk::k_wide8_packet<1, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+}
+
+cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries,
+                                        uint32_t total, const uint32_t* order, unsigned int* counter,
+                                        rtk::DevStatus* st, cudaStream_t stream, int uniform_mode) {
+  if (total == 0) return cudaSuccess;
+  rtk::W8View v;
+  if (!view_of(s, v) || s.top != 0) return cudaErrorInvalidValue;
+  using rtk::ManyBatches;
+  const ManyBatches src{table, entries, order};
+#define RT_W8P(L, AM) run_packet(rtk::k_wide8_packet<L, AM, W8_BLOCK, ManyBatches>, s.words, v, src, counter, total, st, stream)
+  if (s.layout == 0) return uniform_mode == 0 ? RT_W8P(0, 0) : (uniform_mode == 1 ? RT_W8P(0, 1) : RT_W8P(0, 2));
+  return uniform_mode == 0 ? RT_W8P(1, 0) : (uniform_mode == 1 ? RT_W8P(1, 1) : RT_W8P(1, 2));
+#undef RT_W8P
+}
+
 }  // namespace rtl

@@ -44,6 +44,13 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
                             ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream,
                             ctx->tuning.wide8_refill);
       break;
+    case RT_KERNEL_WIDE8_PACKET:
+      if (!scene->d_wide8)
+        return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
+      if (scene->info.top != 0) return fail(ctx, RT_ERR_UNSUPPORTED, "the packet walk takes flat instance lists only");
+      e = rtl::launch_wide8_packet(v, (uint32_t)mode, r, order, hits, n,
+                                   ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream);
+      break;
     default:
       return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
   }
@@ -56,7 +63,7 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
 rt_status check_trace_args(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel) {
   if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null context or scene");
   if ((unsigned)mode > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown mode %d", (int)mode);
-  if ((unsigned)kernel > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown kernel %d", (int)kernel);
+  if ((unsigned)kernel > 3u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown kernel %d", (int)kernel);
   return RT_OK;
 }
 
@@ -203,7 +210,7 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
 
 rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
-  if (kernel != RT_KERNEL_WIDE8) return RT_OK;  // PLAIN and FAST read the packed words directly
+  if (kernel != RT_KERNEL_WIDE8 && kernel != RT_KERNEL_WIDE8_PACKET) return RT_OK;  // PLAIN, FAST: the packed words
   if (scene->d_wide8) return RT_OK;
   std::vector<uint32_t> words(scene->n_words);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -235,7 +235,7 @@ size_t resident_bytes(const rt_server* srv) {
 rt_status rt_server_create(rt_ctx* ctx, const rt_server_desc* desc, rt_server** out) {
   if (!ctx || !desc || !out) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
   *out = nullptr;
-  if (desc->kernel != RT_KERNEL_PLAIN && desc->kernel != RT_KERNEL_FAST && desc->kernel != RT_KERNEL_WIDE8)
+  if ((unsigned)desc->kernel > (unsigned)RT_KERNEL_WIDE8_PACKET)
     return fail(ctx, RT_ERR_INVALID_ARG, "unknown kernel %d", (int)desc->kernel);
   if (desc->slots == 0 || desc->slots > 64) return fail(ctx, RT_ERR_INVALID_ARG, "slots must be 1-64");
   if (desc->launch_rays == 0 || desc->launch_rays > (1u << 26))
@@ -277,7 +277,7 @@ rt_status rt_server_add_scene(rt_server* srv, rt_layout layout, const uint32_t* 
   rt_scene* scene = nullptr;
   rt_status st = rt_scene_upload(ctx, layout, words, n_words, &scene);
   if (st != RT_OK) return st;
-  if (srv->desc.kernel == RT_KERNEL_WIDE8 && (st = rt_scene_prepare(ctx, scene, RT_KERNEL_WIDE8)) != RT_OK) {
+  if (srv->desc.kernel >= RT_KERNEL_WIDE8 && (st = rt_scene_prepare(ctx, scene, RT_KERNEL_WIDE8)) != RT_OK) {
     rt_scene_release(ctx, scene);
     return st;
   }

@@ -5,7 +5,8 @@ Parameters searched (each candidate is one rt_plan, timed as a whole, sort inclu
 
 * kernel -- PLAIN (one thread per ray, a launch per batch), FAST (persistent warps over the
   BVH4-Q8, bit-exact with the reference loop like PLAIN) or WIDE8 (8-wide compressed nodes,
-  watertight f32 test with f64 re-tests);
+  watertight f32 test with f64 re-tests) or WIDE8 walked by warp-wide packets of 32 rays ("wide8p":
+  the same results; flat instance lists only);
 * wavefront width -- the refill threshold: how many lanes of a 32-wide warp must be idle before
   the warp takes more rays (1 keeps every lane busy; 32 hands out whole runs of 32 consecutive
   rays, which keeps a coherent batch's 8 x 4 tiles together);
@@ -24,7 +25,7 @@ import numpy as np
 
 from . import api as A
 
-KERNELS = ("plain", "fast", "wide8")
+KERNELS = ("plain", "fast", "wide8", "wide8p")
 REFILLS = (4, 8, 16, 32)
 ORDERS = ("none", "origin", "octant")
 
@@ -75,9 +76,11 @@ def candidates(kernels=KERNELS, refills=REFILLS, orders=ORDERS) -> list:
     """Every (kernel, refill, order), the usual winners first: unsorted before sorted, the middle
     and widest wavefronts before the rest."""
     pri = {8: 0, 32: 1, 16: 2, 4: 3}
-    grid = [(k, r, o) for k in kernels for r in refills for o in orders if k != "plain"]
+    grid = [(k, r, o) for k in kernels for r in refills for o in orders if k not in ("plain", "wide8p")]
     if "plain" in kernels:  # no ray queue and no sort: one candidate
         grid.append(("plain", 0, orders[0]))
+    if "wide8p" in kernels:  # warps take whole packets of 32 rays: no wavefront width
+        grid += [("wide8p", 32, o) for o in orders]
     return sorted(grid, key=lambda c: (orders.index(c[2]) > 0, pri.get(c[1], 4), kernels.index(c[0])))
 
 

@@ -88,6 +88,7 @@ def test_validation_rejects_unsafe_words():
 def test_tuner_candidates_cover_the_grid_once():
     from renderlab_b200 import tune as T
     c = T.candidates()
-    assert len(c) == len(set(c)) == (len(T.KERNELS) - 1) * len(T.REFILLS) * len(T.ORDERS) + 1
+    assert len(c) == len(set(c)) == (len(T.KERNELS) - 2) * len(T.REFILLS) * len(T.ORDERS) + 1 + len(T.ORDERS)
     assert [x for x in c if x[0] == "plain"] == [("plain", 0, "none")]
+    assert {x[1] for x in c if x[0] == "wide8p"} == {32}
     assert c[0][2] == "none" and c[-1][2] != "none"

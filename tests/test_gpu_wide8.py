@@ -59,21 +59,27 @@ def check_any(got, rays, ref64, what):
     assert len(bad) == 0, f"{what}: {len(bad)} any-hit mismatches; first {bad[:4]}"
 
 
-def traced(engine, layout, words, rays, mode):
+@pytest.fixture(params=["wide8", "wide8p"])
+def w8kernel(request):
+    """Both WIDE8 walks: one ray per lane, and warp-wide packets of 32 rays (flat scenes)."""
+    return request.param
+
+
+def traced(engine, layout, words, rays, mode, kernel="wide8"):
     scene = engine.upload(layout, words)
     try:
         scene.prepare("wide8")
-        return gpu_trace(engine, scene, rays, mode, "wide8")
+        return gpu_trace(engine, scene, rays, mode, kernel)
     finally:
         scene.release()
 
 
 @pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
-def test_wide8_clusters_primary_and_gi(engine, layout):
+def test_wide8_clusters_primary_and_gi(engine, w8kernel, layout):
     mesh, rays = H.small_clusters(60_000, 256, 256)
     prims = [True] if layout == A.LAYOUT_GI else None
     w = product_words(layout, [mesh], S.identity_instances(1), primitives=prims)
-    got = traced(engine, layout, w, rays, A.CLOSEST)
+    got = traced(engine, layout, w, rays, A.CLOSEST, w8kernel)
     ref, ident = O.fp64_trace(w, rays, layout)
     stats = check_closest(layout, got, ref, ident, "primary")
     hit = ref[:, 0] > 0
@@ -81,7 +87,7 @@ def test_wide8_clusters_primary_and_gi(engine, layout):
     prim = ident[hit, 1]
     gi = S.hemisphere_rays(pts, S.triangle_normals(mesh, prim if layout == A.LAYOUT_REFLECTION else ident[hit, 1]),
                            rays[hit, 4:7], 40_000, S.Stream(77))
-    got = traced(engine, layout, w, gi, A.CLOSEST)
+    got = traced(engine, layout, w, gi, A.CLOSEST, w8kernel)
     ref, ident = O.fp64_trace(w, gi, layout)
     stats_gi = check_closest(layout, got, ref, ident, "gi")
     print("wide8 t error (max, mean, ties)", stats, stats_gi)
@@ -103,7 +109,7 @@ def test_wide8_instanced_cubes(engine, layout):
     check_any(got, sun, ref_any, "sun")
 
 
-def test_wide8_edge_rays(engine):
+def test_wide8_edge_rays(engine, w8kernel):
     p, i = H.grid(12)
     mesh = S.Mesh(p, i)
     rays = []
@@ -114,12 +120,12 @@ def test_wide8_edge_rays(engine):
     rays = np.array(rays, np.float32)
     for layout in (A.LAYOUT_GI, A.LAYOUT_REFLECTION):
         w = product_words(layout, [mesh], S.identity_instances(1))
-        got = traced(engine, layout, w, rays, A.CLOSEST)
+        got = traced(engine, layout, w, rays, A.CLOSEST, w8kernel)
         ref, ident = O.fp64_trace(w, rays, layout)
         check_closest(layout, got, ref, ident, f"edge rays layout {layout}")
 
 
-def test_wide8_grid_edges_are_watertight(engine):
+def test_wide8_grid_edges_are_watertight(engine, w8kernel):
     """Rays aimed exactly at shared edges and vertices of a grid: none slips through."""
     p, i = H.grid(16)
     mesh = S.Mesh(p * np.float32(4.0), i)
@@ -128,7 +134,7 @@ def test_wide8_grid_edges_are_watertight(engine):
     rays = S.pack_rays(o, np.tile([0.0, -1.0, 0.0], (len(o), 1)), 0.0, 10.0)
     for layout in (A.LAYOUT_GI, A.LAYOUT_REFLECTION):
         w = product_words(layout, [mesh], S.identity_instances(1))
-        got = traced(engine, layout, w, rays, A.CLOSEST)
+        got = traced(engine, layout, w, rays, A.CLOSEST, w8kernel)
         hit = got[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)
         assert hit.all(), f"{(~hit).sum()} rays slipped through the grid"
 
@@ -146,5 +152,53 @@ def test_wide8_refuses_blas_beyond_its_decode_range(engine):
         rays = np.array([[1.0, 0.25, -1.0, 0.0, 0.0, 0.0, 1.0, 10.0]], np.float32)
         got = gpu_trace(engine, scene, rays, A.CLOSEST, "fast")
         assert got[0, 1] != 0
+    finally:
+        scene.release()
+
+
+def test_packet_walk_needs_a_flat_instance_list(engine):
+    """The packet walk shares one traversal between 32 rays and covers flat instance lists; a
+    scene with a top level is refused, not walked wrongly."""
+    import torch
+    mesh, inst = S.cubes_instanced(8)
+    w = product_words(A.LAYOUT_REFLECTION, [mesh], inst)
+    assert w[1] != 0
+    scene = engine.upload(A.LAYOUT_REFLECTION, w)
+    try:
+        scene.prepare("wide8")
+        rays = torch.from_numpy(H.small_cubes(8, 16, 16)[1]).cuda()
+        with pytest.raises(A.RtError, match="UNSUPPORTED"):
+            engine.trace(scene, rays, A.CLOSEST, "wide8p")
+    finally:
+        scene.release()
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_packet_walk_matches_the_per_ray_walk(engine, layout):
+    """Per ray, the packet walk finds the per-ray walk's hit: ids equal, t within the f64
+    band (the t of a winner the per-ray walk accepted in f32 may come back refined in f64), for
+    coherent primaries, incoherent GI rays, a permutation and batches with mixed modes."""
+    import torch
+    mesh, rays = H.small_clusters(60_000, 256, 256)
+    prims = [True] if layout == A.LAYOUT_GI else None
+    w = product_words(layout, [mesh], S.identity_instances(1), primitives=prims)
+    scene = engine.upload(layout, w)
+    try:
+        scene.prepare("wide8")
+        rnd = H.random_rays(30_000, -120.0, 120.0, seed=4, tmax=400.0)
+        for batch in (rays, rnd):
+            d = torch.from_numpy(batch).cuda()
+            order = engine.order(scene, d, "origin")
+            a = engine.trace(scene, d, A.CLOSEST, "wide8").cpu().numpy().view(np.uint32)
+            for kw in ({}, {"order": order}):
+                b = engine.trace(scene, d, A.CLOSEST, "wide8p", **kw).cpu().numpy().view(np.uint32)
+                ids = slice(1, 3) if layout == A.LAYOUT_REFLECTION else slice(1, 5)
+                assert np.array_equal(a[:, ids], b[:, ids])
+                ta, tb = a[:, 0].view(np.float32), b[:, 0].view(np.float32)
+                assert np.all(np.abs(ta - tb) <= 2e-5 * np.abs(ta))
+            flags_a = engine.trace(scene, d, A.ANY_CASTERS, "wide8").cpu().numpy()
+            got = engine.trace_batches(scene, [(d[:1000], A.ANY_CASTERS), (d[1000:], A.CLOSEST)], "wide8p")
+            assert np.array_equal(got[0].cpu().numpy(), flags_a[:1000])
+            assert np.array_equal(got[1].cpu().numpy().view(np.uint32)[:, ids], a[1000:, ids])
     finally:
         scene.release()
