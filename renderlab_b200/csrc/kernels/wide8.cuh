@@ -11,9 +11,9 @@
 //   shear matrix; an edge function that rounds to zero is recomputed in double. Shared vertices
 //   transform identically, so a ray never slips between two triangles.
 // * FP64: candidates whose f32 result is uncertain -- within 8e-6 relative of the current best
-//   (a near tie), of tmin or tmax, or within 1e-5 of an edge -- are re-intersected with the f64
-//   Möller-Trumbore test over the source triangle in the packed words, in the exact arithmetic
-//   of the f64 reference (crates/asset/src/cluster_bvh/reference.rs:121-158), and ties resolve
+//   (a near tie), of tmin or tmax, or within the f32 edge functions' error bound of an edge -- are
+//   re-intersected with the f64 Möller-Trumbore test over the source triangle in the packed
+//   words, in the exact arithmetic of the f64 reference (crates/asset/src/cluster_bvh/reference.rs:121-158), and ties resolve
 //   on (t, instance, triangle) as it does.
 #pragma once
 #include "plain.cuh"
@@ -179,7 +179,15 @@ RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, 
   const float V = w8_edge(A.x, A.y, C.x, C.y);  // opposite v1
   const float W = w8_edge(B.x, B.y, A.x, A.y);  // opposite v2
   const float sum = __fadd_rn(__fadd_rn(fabsf(U), fabsf(V)), fabsf(W));
-  const float lim = __fmul_rn(W8_EDGE, sum);
+  // How far an f32 edge function may be from the exact one. A projected coordinate is off by at
+  // most eA = 8 u |v - o| (the rounding of v - o, of the shear factor and of the fma; |shear| <= 1)
+  // plus twice the origin's own error; an edge function of coordinates up to pm is then off by at
+  // most 4 pm eA + 2 eA^2 + 4 u pm^2 (taken here with margin). For a small triangle far from the
+  // origin this dominates the relative part, W8_EDGE * sum: such hits near an edge are re-tested.
+  const float pm = fmaxf(fmaxf(fmaxf(fabsf(A.x), fabsf(A.y)), fmaxf(fabsf(B.x), fabsf(B.y))),
+                         fmaxf(fabsf(C.x), fabsf(C.y)));
+  const float eA = fmaf(8.0f * W8_U, dmax, 2.0f * R.oerr);
+  const float lim = fmaf(W8_EDGE, sum, fmaf(fmaf(3.0f, eA, 5.0f * pm), eA, 5.0f * W8_U * pm * pm));
   const bool neg = U < 0.0f || V < 0.0f || W < 0.0f, pos = U > 0.0f || V > 0.0f || W > 0.0f;
   int kind = 1;
   if (neg && pos) {

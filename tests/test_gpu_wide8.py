@@ -202,3 +202,40 @@ def test_packet_walk_matches_the_per_ray_walk(engine, layout):
             assert np.array_equal(got[1].cpu().numpy().view(np.uint32)[:, ids], a[1000:, ids])
     finally:
         scene.release()
+
+
+def test_wide8_far_small_triangles_near_edges(engine, w8kernel):
+    """Isolated small triangles (0.05 units) 200 units down the view axis and 50 units to its
+    side, rays aimed within 1e-6 to 1e-3 of an edge, inside and outside. The shear's rounding grows
+    with the lateral offset: here an f32 edge function can be off by ~1e-4 of the edge functions'
+    sum, more than a margin relative to that sum allows, so these rays must be re-tested in f64
+    and agree with the FP64 oracle (a hit its oracle triangle, a miss a miss) on every ray."""
+    rng = np.random.default_rng(3)
+    size, tris = 0.05, []
+    for k in range(64):
+        x0, y0 = 40.0 + (k % 8) * 2 * size, -30.0 + (k // 8) * 2 * size
+        z = rng.uniform(-0.01, 0.01)
+        tris.append([[x0, y0, z], [x0 + size, y0 + 0.2 * size, z + 0.003], [x0 + 0.1 * size, y0 + size, z - 0.003]])
+    p = np.array(tris, np.float32).reshape(-1, 3)
+    mesh = S.Mesh(p, np.arange(len(p), dtype=np.uint32))
+    n = 8192
+    t = rng.uniform(0.05, 0.95, n)
+    q = rng.integers(0, 64, n)
+    e = rng.integers(0, 3, n)  # which edge
+    v0, v1 = p[3 * q + e].astype(np.float64), p[3 * q + (e + 1) % 3].astype(np.float64)
+    other = p[3 * q + (e + 2) % 3].astype(np.float64)
+    on_edge = v0 * (1 - t)[:, None] + v1 * t[:, None]
+    inward = other - on_edge
+    inward /= np.linalg.norm(inward, axis=1, keepdims=True)
+    off = rng.choice([-1.0, 1.0], n) * size * 10.0 ** rng.uniform(-6, -3, n)
+    b = on_edge + inward * off[:, None]
+    o = np.array([0.0, 0.0, -200.0])
+    d = b - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    rays = S.pack_rays(np.tile(o, (n, 1)), d, 0.0, 1e30)
+    for layout in (A.LAYOUT_GI, A.LAYOUT_REFLECTION):
+        w = product_words(layout, [mesh], S.identity_instances(1))
+        got = traced(engine, layout, w, rays, A.CLOSEST, w8kernel)
+        ref, ident = O.fp64_trace(w, rays, layout)
+        check_closest(layout, got, ref, ident, f"near edges, layout {layout}")
+        assert 0.3 < (ref[:, 0] > 0).mean() < 0.7
