@@ -165,6 +165,21 @@ typedef enum rt_ray_order {
  * rt_ctx_reserve). Asynchronous on `stream`. */
 rt_status rt_order_rays(rt_ctx* ctx, const rt_scene* scene, const rt_ray* d_rays, uint32_t n, rt_ray_order key,
                         uint32_t* d_order, void* stream);
+/* GPU refit of the BLAS that instance `instance` uses (near_field::refit_bvh, near_field.rs:445-478,
+ * on the device): the same vertices and triangles at new positions. GI layout: d_positions (3
+ * floats a vertex, n_positions of them) replaces the BLAS's position words. Reflection layout: the
+ * pre-edged triangles are rewritten from d_positions through d_indices (the mesh's triangle list,
+ * as given to rt_blas_build). The node boxes are refit bottom-up with the host refit's arithmetic:
+ * the words equal those of rt_blas_refit + rt_pack_scene. Asynchronous on `stream` (the first call
+ * per BLAS reads its topology synchronously). Every instance of the BLAS sees the change. The
+ * instance records and the top level are not touched: when the geometry leaves its records' world
+ * boxes, rewrite them with rt_scene_update_records, as the reference refits and re-places its
+ * instances. The scene's derived WIDE8 layout is dropped (rt_scene_prepare builds it again). */
+rt_status rt_scene_refit(rt_ctx* ctx, rt_scene* scene, uint32_t instance, const float* d_positions,
+                         uint32_t n_positions, const uint32_t* d_indices, uint32_t n_indices, void* stream);
+/* Copies words [first, first + n) of the scene's device buffer to host memory (synchronous). */
+rt_status rt_scene_read_words(rt_ctx* ctx, const rt_scene* scene, size_t first, size_t n, uint32_t* out);
+
 /* ---- Many batches in one launch ----------------------------------------------------------
  * Uneven ray batches of one scene, each with its own buffers and mode, traced by ONE persistent
  * launch that hands out rays from the concatenation of the batches. Per batch, the results are

@@ -83,7 +83,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
-           "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
+           "rt_scene_refit", "rt_scene_read_words", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
            "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
@@ -128,6 +128,8 @@ def lib() -> ctypes.CDLL:
     L.rt_plan_launch.argtypes = [_vp, _vp]
     L.rt_plan_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.rt_plan_destroy.argtypes = [_vp]
+    L.rt_scene_refit.argtypes = [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]
+    L.rt_scene_read_words.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _u32p]
     L.rt_server_create.argtypes = [_vp, ctypes.POINTER(RtServerDesc), ctypes.POINTER(_vp)]
     L.rt_server_add_scene.argtypes = [_vp, ctypes.c_int, _u32p, ctypes.c_size_t, _u32p]
     L.rt_server_remove_scene.argtypes = [_vp, ctypes.c_uint32]
@@ -307,6 +309,23 @@ class Scene:
     def prepare(self, kernel: str = "wide8"):
         """Build the derived layout `kernel` reads (the 8-wide BVH for "wide8")."""
         self.engine._check(lib().rt_scene_prepare(self.engine.ctx, self.handle, KERNELS[kernel]))
+
+    def refit(self, instance: int, positions, indices=None, stream=None):
+        """rt_scene_refit: new positions (CUDA float32 tensor (V, 3)) for the BLAS of `instance`;
+        the reflection layout also takes the mesh's triangle list (CUDA int32/uint32 tensor)."""
+        import torch
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        n_idx = 0 if indices is None else int(indices.numel())
+        self.engine._check(lib().rt_scene_refit(self.engine.ctx, self.handle, instance, positions.data_ptr(),
+                                                int(positions.shape[0]), indices.data_ptr() if indices is not None else None,
+                                                n_idx, s))
+
+    def words(self, first: int = 0, n: int = -1) -> np.ndarray:
+        """A host copy of the scene's device words [first, first + n)."""
+        n = self.n_words - first if n < 0 else n
+        out = np.zeros(n, np.uint32)
+        self.engine._check(lib().rt_scene_read_words(self.engine.ctx, self.handle, first, n, _np_ptr(out, _u32p)))
+        return out
 
     def update_records(self, words):
         w = np.ascontiguousarray(words, np.uint32)

@@ -5,6 +5,8 @@
 
 #include <atomic>
 #include <cstdarg>
+#include <map>
+#include <vector>
 #include <cstdio>
 #include <mutex>
 #include <string>
@@ -12,6 +14,16 @@
 #include "../../include/rt_trace.h"
 #include "host/host.hpp"
 #include "launch.hpp"
+
+// Per BLAS of a scene, what rt_scene_refit needs about its (fixed) topology: its nodes ordered
+// by height above the leaves, and where each height starts.
+struct RefitLevels {
+  uint32_t node_count = 0;
+  uint32_t tri_count = 0;           // reflection layout: packed triangles of the BLAS
+  uint32_t position_count = 0;      // GI layout: position records of the BLAS
+  std::vector<uint32_t> level_start;  // level h: d_order[level_start[h], level_start[h + 1])
+  uint32_t* d_order = nullptr;
+};
 
 struct rt_scene {
   uint32_t layout = 0;
@@ -22,6 +34,7 @@ struct rt_scene {
   void* d_wide8 = nullptr;
   size_t wide8_bytes = 0;
   size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
+  std::map<uint32_t, RefitLevels> refit;  // by the BLAS's node base word
 };
 
 struct rt_blas {

@@ -251,6 +251,7 @@ rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene) {
   cudaSetDevice(ctx->device);
   cudaFree(scene->d_words);
   cudaFree(scene->d_wide8);
+  for (auto& kv : scene->refit) cudaFree(kv.second.d_order);
   ctx->scene_bytes -= scene->device_bytes;
   delete scene;
   return RT_OK;
