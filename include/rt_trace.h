@@ -180,6 +180,30 @@ rt_status rt_scene_refit(rt_ctx* ctx, rt_scene* scene, uint32_t instance, const 
 /* Copies words [first, first + n) of the scene's device buffer to host memory (synchronous). */
 rt_status rt_scene_read_words(rt_ctx* ctx, const rt_scene* scene, size_t first, size_t n, uint32_t* out);
 
+/* ---- The GI cache's ray producers --------------------------------------------------------
+ * A cache cell (32 bytes) as gi_cache.wgsl keeps it: query point, cell edge, octahedral normal
+ * (pack2x16snorm) and the key word whose high 24 bits turn the cell's directions. */
+typedef struct rt_gi_cell {
+  float q[3];
+  float edge;
+  uint32_t normal;
+  uint32_t key_b;
+  uint32_t pad[2];
+} rt_gi_cell;
+#define RT_GI_DIRECTIONS 64u /* rays a cell */
+#define RT_GI_ROTATE 4u      /* GI_F_ROTATE: turn each cell's directions by its key */
+/* The cells' fixed directions as rays (gi_direction about gi_basis of the normal, from the
+ * query point offset along it by gi_origin_offset; tmin 0, tmax 1e20): ray k of cell c is
+ * d_rays[c * 64 + k] (gi_cache.wgsl:1046-1068, gi_cells.wgsl:463-487). */
+rt_status rt_gi_cell_rays(rt_ctx* ctx, const rt_gi_cell* d_cells, uint32_t n_cells, uint32_t flags, rt_ray* d_rays,
+                          void* stream);
+/* The same rays traced against a GI-layout scene by the FAST kernel, generated in its ray refill
+ * (no ray buffer): RT_CLOSEST gives the gather's rt_gi_hit per item (gi_gather_software.wgsl:89-94),
+ * RT_ANY_SKY one uint32 per item, 1 when blocked (gi_ray's visibility, gi_cache.wgsl:1562-1575,
+ * keeps the negation as a bit). Results at d_hits[c * 64 + k]. */
+rt_status rt_trace_gi_cells(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, const rt_gi_cell* d_cells,
+                            uint32_t n_cells, uint32_t flags, void* d_hits, void* stream);
+
 /* ---- Many batches in one launch ----------------------------------------------------------
  * Uneven ray batches of one scene, each with its own buffers and mode, traced by ONE persistent
  * launch that hands out rays from the concatenation of the batches. Per batch, the results are

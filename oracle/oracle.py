@@ -74,6 +74,8 @@ def lib():
                                    _u64p, ctypes.c_int]
         L.orc_rs_trace_counts.argtypes = [_u32p, _f32p, ctypes.c_uint32, ctypes.c_int, ctypes.c_int,
                                           _u32p, _u64p]
+        L.orc_gi_cell_rays.argtypes = [_u32p, ctypes.c_uint32, ctypes.c_int, _f32p]
+        L.orc_gi_cell_rays.restype = None
         L.orc_fp64_trace.argtypes = [_u32p, ctypes.c_int, _f32p, ctypes.c_uint32, ctypes.c_int, _f64p,
                                      _u32p, ctypes.c_int]
         _lib = L
@@ -250,6 +252,15 @@ def rs_trace_counts(words, rays, any_hit=False, bvh2=False):
     lib().orc_rs_trace_counts(_p(w, _u32p), _p(r, _f32p), len(r), int(any_hit), int(bvh2),
                               _p(hits, _u32p), _p(cnt, _u64p))
     return hits, cnt
+
+
+def gi_cell_rays(cells, rotate=False):
+    """The GI cache cells' fixed-direction rays (gi_cache.wgsl gi_direction / gi_origin_offset):
+    cells (n, 8) uint32 records (q xyz, edge, packed normal, key_b, 0, 0); (n * 64, 8) float32."""
+    c = _c(cells, np.uint32).reshape(-1, 8)
+    out = np.zeros((len(c) * 64, 8), np.float32)
+    lib().orc_gi_cell_rays(_p(c, _u32p), len(c), int(bool(rotate)), _p(out, _f32p))
+    return out
 
 
 def fp64_trace(words, rays, layout, any_hit=False, threads=None):

@@ -31,6 +31,7 @@ ORDERS = {"none": 0, "origin": 1, "octant": 2, "direction": 3}
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "LAYOUT", 3: "OOM", 4: "STACK_OVERFLOW", 5: "TIMEOUT",
           6: "CUDA", 7: "BUSY", 8: "UNSUPPORTED"}
 GI_HIT_WORDS, RS_HIT_WORDS = 10, 5
+GI_DIRECTIONS, GI_ROTATE = 64, 4
 MISS = 0xFFFFFFFF
 
 _u32p = ctypes.POINTER(ctypes.c_uint32)
@@ -83,7 +84,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
-           "rt_scene_refit", "rt_scene_read_words", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
+           "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
            "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
@@ -129,6 +130,8 @@ def lib() -> ctypes.CDLL:
     L.rt_plan_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint64)]
     L.rt_plan_destroy.argtypes = [_vp]
     L.rt_scene_refit.argtypes = [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]
+    L.rt_gi_cell_rays.argtypes = [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]
+    L.rt_trace_gi_cells.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]
     L.rt_scene_read_words.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _u32p]
     L.rt_server_create.argtypes = [_vp, ctypes.POINTER(RtServerDesc), ctypes.POINTER(_vp)]
     L.rt_server_add_scene.argtypes = [_vp, ctypes.c_int, _u32p, ctypes.c_size_t, _u32p]
@@ -539,6 +542,29 @@ class Engine:
         self._check(lib().rt_plan_create(self.ctx, scene.handle, arr, len(batches), ctypes.byref(desc), ctypes.byref(h)))
         return Plan(self, scene, h, outs, [b[0] for b in batches], dict(kernel=kernel, refill=refill, order=order,
                                                                           graph=graph))
+
+    def gi_cell_rays(self, cells, rotate: bool = False, stream=None):
+        """The GI cache cells' 64 fixed-direction rays each: cells (n, 8) int32 CUDA tensor of
+        rt_gi_cell records; returns (n * 64, 8) float32."""
+        import torch
+        n = cells.shape[0]
+        rays = torch.empty((n * GI_DIRECTIONS, 8), dtype=torch.float32, device=cells.device)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self._check(lib().rt_gi_cell_rays(self.ctx, cells.data_ptr(), n, GI_ROTATE if rotate else 0, rays.data_ptr(), s))
+        return rays
+
+    def trace_gi_cells(self, scene: Scene, cells, mode: int = CLOSEST, rotate: bool = False, hits=None, stream=None):
+        """The cells' rays generated inside the FAST kernel and traced (GI layout): rt_gi_hit per
+        item for CLOSEST, a blocked flag per item for ANY_SKY."""
+        import torch
+        n = cells.shape[0] * GI_DIRECTIONS
+        words = hit_words(scene.layout, mode)
+        if hits is None:
+            hits = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=cells.device)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self._check(lib().rt_trace_gi_cells(self.ctx, scene.handle, mode, cells.data_ptr(), cells.shape[0],
+                                            GI_ROTATE if rotate else 0, hits.data_ptr(), s))
+        return hits
 
     def order(self, scene: Scene, rays, key: str = "octant", out=None, stream=None):
         """A permutation of `rays` (CUDA tensor) grouping alike rays; int32 CUDA tensor."""

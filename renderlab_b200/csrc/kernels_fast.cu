@@ -1,6 +1,7 @@
 // Launchers for the FAST kernels: persistent grids sized to fill every SM once.
 #include <cuda_runtime.h>
 
+#include "kernels/cells.cuh"
 #include "kernels/fast.cuh"
 #include "launch.hpp"
 
@@ -75,6 +76,17 @@ cudaError_t launch_fast_batches(const SceneView& s, const rtk::BatchEntry* table
   if (uniform_mode == 0) return run(rtk::k_rs_fast<0, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
   if (uniform_mode == 1) return run(rtk::k_rs_fast<1, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
   return run(rtk::k_rs_fast<2, FAST_BLOCK, ManyBatches>, s, src, total, counter, st, stream, refill);
+}
+
+cudaError_t launch_fast_cells(const SceneView& s, uint32_t mode, const void* cells, uint32_t n_cells, uint32_t rotate,
+                              void* hits, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
+  const uint32_t items = n_cells * rtk::GI_DIRECTIONS;
+  if (items == 0) return cudaSuccess;
+  if (s.layout != 0) return cudaErrorInvalidValue;
+  using rtk::CellRays;
+  const CellRays src{static_cast<const rtk::GiCell*>(cells), rotate, hits};
+  if (mode == 0) return run(rtk::k_gi_fast<0, FAST_BLOCK, CellRays>, s, src, items, counter, st, stream, refill);
+  return run(rtk::k_gi_fast<1, FAST_BLOCK, CellRays>, s, src, items, counter, st, stream, refill);
 }
 
 }  // namespace rtl

@@ -52,6 +52,12 @@ cudaError_t launch_wide8_packet(const SceneView& s, uint32_t mode, const float4*
 cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries,
                                         uint32_t total, const uint32_t* order, unsigned int* counter,
                                         rtk::DevStatus* st, cudaStream_t stream, int uniform_mode);
+// The GI cache's cell ray producers (kernels/cells.cuh): 64 rays a cell written to `rays`
+// (kernels_cells.cu), or generated inside the FAST GI kernel and traced (mode 0 closest, else sky
+// any hit), results at the item index (kernels_fast.cu).
+cudaError_t launch_cell_rays(const void* cells, uint32_t n_cells, uint32_t rotate, float4* rays, cudaStream_t stream);
+cudaError_t launch_fast_cells(const SceneView& s, uint32_t mode, const void* cells, uint32_t n_cells, uint32_t rotate,
+                              void* hits, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
 // Ray ordering (kernels_order.cu): scratch holds the keys, the unsorted indices and the radix
 // sort's temporary storage.
 size_t order_scratch_bytes(uint32_t n);

@@ -504,3 +504,31 @@ rt_status rt_tlas_refit(uint32_t* nodes, size_t n_words, const float* boxes, uin
 }
 
 }  // extern "C"
+
+rt_status rt_gi_cell_rays(rt_ctx* ctx, const rt_gi_cell* d_cells, uint32_t n_cells, uint32_t flags, rt_ray* d_rays,
+                          void* stream) {
+  if (!ctx || (n_cells && (!d_cells || !d_rays))) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if (n_cells > (1u << 25)) return fail(ctx, RT_ERR_INVALID_ARG, "at most 2^25 cells a call");
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, rtl::launch_cell_rays(d_cells, n_cells, (flags & RT_GI_ROTATE) ? 1u : 0u, reinterpret_cast<float4*>(d_rays),
+                                     static_cast<cudaStream_t>(stream)));
+  return RT_OK;
+}
+
+rt_status rt_trace_gi_cells(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, const rt_gi_cell* d_cells,
+                            uint32_t n_cells, uint32_t flags, void* d_hits, void* stream) {
+  rt_status s = check_trace_args(ctx, scene, mode, RT_KERNEL_FAST);
+  if (s != RT_OK) return s;
+  if (scene->layout != RT_LAYOUT_GI) return fail(ctx, RT_ERR_INVALID_ARG, "the cell producers trace GI-layout scenes");
+  if (n_cells && (!d_cells || !d_hits)) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if (n_cells > (1u << 25)) return fail(ctx, RT_ERR_INVALID_ARG, "at most 2^25 cells a call");
+  if (reinterpret_cast<uintptr_t>(d_hits) % 4 != 0) return fail(ctx, RT_ERR_INVALID_ARG, "hits must be 4-byte aligned");
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  cudaError_t e = rtl::launch_fast_cells(view_of(scene), (uint32_t)mode, d_cells, n_cells, (flags & RT_GI_ROTATE) ? 1u : 0u,
+                                         d_hits, ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status,
+                                         static_cast<cudaStream_t>(stream), ctx->tuning.fast_refill);
+  if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "cell traversal: %s", cudaGetErrorString(e));
+  ctx->rays += (uint64_t)n_cells * RT_GI_DIRECTIONS;
+  ctx->launches += 1;
+  return RT_OK;
+}

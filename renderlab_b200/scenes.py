@@ -247,6 +247,29 @@ def uneven_batches(n_batches: int = 64, lo: float = 1e3, hi: float = 2e6, half: 
 RAY_DTYPE = np.dtype([("o", np.float32, 3), ("tmin", np.float32), ("d", np.float32, 3), ("tmax", np.float32)])
 
 
+def pack_normal(n: np.ndarray) -> np.ndarray:
+    """Unit normals (N, 3) in the GI cache's octahedral pack2x16snorm word (gi_cache.wgsl
+    gi_pack_normal)."""
+    n = np.asarray(n, np.float64)
+    p = n[:, :2] / np.abs(n).sum(axis=1, keepdims=True)
+    sign = np.where(p >= 0.0, 1.0, -1.0)
+    q = np.where(n[:, 2:3] >= 0.0, p, (1.0 - np.abs(p[:, ::-1])) * sign)
+    s = np.round(np.clip(q, -1.0, 1.0) * 32767.0).astype(np.int64) & 0xFFFF
+    return (s[:, 0] | (s[:, 1] << 16)).astype(np.uint32)
+
+
+def gi_cells(points: np.ndarray, normals: np.ndarray, edge: float, stream: Stream) -> np.ndarray:
+    """rt_gi_cell records (N, 8) uint32 at the given points: query point, cell edge, packed
+    normal, a random key word."""
+    n = len(points)
+    out = np.zeros((n, 8), np.uint32)
+    out[:, 0:3] = np.asarray(points, np.float32).view(np.uint32)
+    out[:, 3] = np.float32(edge).view(np.uint32)
+    out[:, 4] = pack_normal(normals)
+    out[:, 5] = (stream.raw(n) >> np.uint64(32)).astype(np.uint32)
+    return out
+
+
 def pack_rays(o, d, tmin, tmax) -> np.ndarray:
     """(n, 8) float32 records: origin xyz, tmin, direction xyz, tmax (the 32-byte rt_ray)."""
     n = len(o)

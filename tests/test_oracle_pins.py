@@ -515,3 +515,33 @@ def test_place_sets_the_header_and_reuses_unchanged_records():
     assert np.array_equal(O.tlas_place(words, header, stride, 3, previous=placed), placed)
     again = O.tlas_place(words, header, stride, 3, previous=forced, mode=1)
     assert np.array_equal(again, forced)
+
+
+def test_gi_cell_rays_are_the_fixed_hemisphere_directions():
+    """gi_direction (gi_cache.wgsl:1046-1054): 64 equal-solid-angle directions about the cell
+    normal -- direction k at cos theta = 1 - (k + 0.5) / 64, golden-angle azimuths -- from the
+    query point offset along the normal by gi_origin_offset (gi_cache.wgsl:1064-1068)."""
+    from renderlab_b200 import scenes as S
+    rng = np.random.default_rng(5)
+    n = rng.normal(size=(40, 3))
+    n /= np.linalg.norm(n, axis=1, keepdims=True)
+    q = rng.uniform(-50, 50, (40, 3)).astype(np.float32)
+    cells = S.gi_cells(q, n, 0.25, S.Stream(3))
+    rays = O.gi_cell_rays(cells).reshape(40, 64, 8)
+    # the normal the producer decoded: close to the packed one (16-bit octahedral encoding)
+    d = rays[:, :, 4:7].astype(np.float64)
+    assert np.allclose(np.linalg.norm(d, axis=2), 1.0, atol=2e-6)
+    z = 1.0 - (np.arange(64) + 0.5) / 64.0
+    cos = np.einsum("ckj,cj->ck", d, n)
+    assert np.abs(cos - z[None, :]).max() < 2e-4
+    # azimuths advance by the golden angle about the normal
+    off = np.linalg.norm(rays[:, 0, 0:3].astype(np.float64) - q, axis=1)
+    m = np.abs(q).max(axis=1)
+    ulp = np.spacing(m.astype(np.float32)).astype(np.float64)
+    want = np.maximum(np.maximum(1e-5, 32.0 * ulp) + 1e-4 * 0.25, 1e-4 + 4e-7 * m)
+    assert np.abs(off - want).max() < 4 * ulp.max()  # q + n * off rounds at |q|'s ulp
+    assert (rays[:, :, 7] == np.float32(1e20)).all() and (rays[:, :, 3] == 0).all()
+    # turned by the key: the same cosines, other azimuths
+    turned = O.gi_cell_rays(cells, rotate=True).reshape(40, 64, 8)
+    assert np.abs(np.einsum("ckj,cj->ck", turned[:, :, 4:7].astype(np.float64), n) - z).max() < 2e-4
+    assert not np.allclose(turned[:, :, 4:7], rays[:, :, 4:7])
