@@ -38,7 +38,9 @@ typedef enum rt_status {
 /* The two packed layouts. */
 typedef enum rt_layout {
   RT_LAYOUT_GI = 0,         /* gi_geometry: 16-word header, 32-word instances (src/gi_bvh.rs:19-25) */
-  RT_LAYOUT_REFLECTION = 1  /* rl_geometry: 8-word header, 24-word instances (reflection_software.rs:38-42) */
+  RT_LAYOUT_REFLECTION = 1, /* rl_geometry: 8-word header, 24-word instances (reflection_software.rs:38-42) */
+  RT_LAYOUT_REFLECTION_BVH2 = 2 /* the legacy median BVH2 reflection layout (reflection_software.rs:170-264,
+                                   reflections_software.wgsl), as geometry dumps carry it; PLAIN kernel only */
 } rt_layout;
 
 /* Query modes: gi_traverse's mode argument (gi_rays_software.wgsl:214-217). For the reflection

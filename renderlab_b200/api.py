@@ -24,7 +24,7 @@ import numpy as np
 
 LIB_PATH = Path(__file__).resolve().parent / "_lib" / "librt_trace.so"
 
-LAYOUT_GI, LAYOUT_REFLECTION = 0, 1
+LAYOUT_GI, LAYOUT_REFLECTION, LAYOUT_REFLECTION_BVH2 = 0, 1, 2
 CLOSEST, ANY_SKY, ANY_CASTERS = 0, 1, 2
 KERNELS = {"plain": 0, "fast": 1, "wide8": 2, "wide8p": 3}
 ORDERS = {"none": 0, "origin": 1, "octant": 2, "direction": 3}

@@ -27,8 +27,10 @@ inline void need(bool ok, const char* what) {
 // Walks one tree from `root` with an explicit stack. visit(node) returns its children; the
 // ordering rule (child < parent for a BLAS, child > parent for a top level) makes the walk
 // finite; `seen` rejects a node reachable twice.
+// order: +1 children below their parent, -1 above it, 0 any order (reachable-once alone keeps
+// the walk finite).
 template <class Children>
-uint32_t walk(uint32_t root, bool children_below, size_t max_nodes, Children&& children) {
+uint32_t walk(uint32_t root, int order, size_t max_nodes, Children&& children) {
   std::vector<uint8_t> seen;
   std::vector<std::pair<uint32_t, uint32_t>> stack;  // (id, depth)
   stack.push_back({root, 0});
@@ -50,7 +52,7 @@ uint32_t walk(uint32_t root, bool children_below, size_t max_nodes, Children&& c
     for (int k = 0; k < n; ++k) {
       uint32_t c = kids[k];
       if (c == EMPTY) continue;
-      if (!(c & LEAF)) need(children_below ? c < id : c > id, "tree children out of order");
+      if (!(c & LEAF) && order != 0) need(order > 0 ? c < id : c > id, "tree children out of order");
       stack.push_back({c, depth + 1});
     }
   }
@@ -60,7 +62,7 @@ uint32_t walk(uint32_t root, bool children_below, size_t max_nodes, Children&& c
 void check_top(const uint32_t* w, size_t n, size_t base, uint32_t root, uint32_t count, SceneInfo& info) {
   need(base < n, "top level base out of range");
   size_t max_nodes = (n - base) / 32;
-  info.max_top_depth = walk(root, false, max_nodes, [&](uint32_t id, uint32_t* kids) -> int {
+  info.max_top_depth = walk(root, -1, max_nodes, [&](uint32_t id, uint32_t* kids) -> int {
     if (id & LEAF) {
       need((id & ~LEAF) < count, "top level leaf names a missing instance");
       return 0;
@@ -98,7 +100,7 @@ bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& inf
         const size_t nodes = r[18], leaves = r[19], positions = r[20], indices = r[21], prim = r[28];
         need(nodes <= n, "GI node base out of range");
         size_t max_nodes = (n - nodes) / 16;
-        uint32_t depth = walk(r[22], true, max_nodes, [&](uint32_t id, uint32_t* kids) -> int {
+        uint32_t depth = walk(r[22], 1, max_nodes, [&](uint32_t id, uint32_t* kids) -> int {
           if (id & LEAF) {
             size_t l = leaves + 2 * (size_t)(id & ~LEAF);
             need(l + 2 <= n, "GI leaf record out of range");
@@ -140,7 +142,7 @@ bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& inf
         const size_t nodes = r[18] & ~3u, tris = r[19] & ~3u;
         need(nodes <= n, "reflection node base out of range");
         size_t max_nodes = (n - nodes) / 16;
-        uint32_t depth = walk(r[20], true, max_nodes, [&](uint32_t id, uint32_t* kids) -> int {
+        uint32_t depth = walk(r[20], 1, max_nodes, [&](uint32_t id, uint32_t* kids) -> int {
           if (id & LEAF) {
             size_t start = (id & ~LEAF) >> 4, cnt = id & 15u;
             need(tris + 12 * (start + cnt) <= n, "reflection triangles out of range");
@@ -153,6 +155,47 @@ bool validate_scene(uint32_t layout, const uint32_t* w, size_t n, SceneInfo& inf
           return 4;
         });
         info.max_blas_depth = std::max(info.max_blas_depth, depth);
+      }
+    } else if (layout == 2) {
+      // The legacy median BVH2 reflection layout (reflection_software.rs:170-264): 16-word nodes
+      // with two boxes and children at words 12-13, leaves LEAF | first << 3 | count.
+      need(n >= 8, "reflection buffer shorter than its header");
+      const uint32_t count = w[0];
+      need(8 + 24 * (size_t)count <= n, "reflection instance records past the buffer");
+      info.instances = count;
+      info.top = w[1];
+      info.root = w[2];
+      auto bvh2 = [&](size_t base, uint32_t root, bool top, size_t tris) -> uint32_t {
+        need(base <= n, "BVH2 node base out of range");
+        return walk(root, 0, (n - base) / 16, [&](uint32_t id, uint32_t* kids) -> int {
+          if (id & LEAF) {
+            if (top) {
+              need((id & ~LEAF) < count, "top level leaf names a missing instance");
+            } else {
+              const size_t start = (id & ~LEAF) >> 3, cnt = id & 7u;
+              need(tris + 12 * (start + cnt) <= n, "reflection triangles out of range");
+              info.triangles += cnt;
+            }
+            return 0;
+          }
+          const uint32_t* node = w + base + 16 * (size_t)id;
+          kids[0] = node[12], kids[1] = node[13], kids[2] = kids[3] = EMPTY;
+          if (!top) info.nodes += 1;
+          return 4;
+        });
+      };
+      if (info.top != 0 && count > 0) info.max_top_depth = bvh2(info.top & ~3u, info.root, true, 0);
+      std::map<std::array<uint32_t, 6>, bool> done;
+      for (uint32_t i = 0; i < count; ++i) {
+        const uint32_t* r = w + 8 + 24 * (size_t)i;
+        for (int a = 0; a < 3; ++a) {
+          info.world.lo[a] = lo_of(info.world.lo[a], as_float(r[12 + a]));
+          info.world.hi[a] = hi_of(info.world.hi[a], as_float(r[15 + a]));
+        }
+        std::array<uint32_t, 6> key = {r[18] & ~3u, r[19] & ~3u, r[20], 0, 0, 0};
+        if (done.count(key)) continue;
+        done[key] = true;
+        info.max_blas_depth = std::max(info.max_blas_depth, bvh2(r[18] & ~3u, r[20], false, r[19] & ~3u));
       }
     } else {
       need(false, "unknown layout");

@@ -1,4 +1,5 @@
 // Launchers for the PLAIN kernels and the arithmetic self-test.
+#include "kernels/bvh2.cuh"
 #include "kernels/plain.cuh"
 #include "launch.hpp"
 
@@ -31,9 +32,12 @@ cudaError_t launch_plain(const SceneView& s, uint32_t mode, const float4* rays, 
     if (mode == 0) rtk::k_gi_plain<0><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
     else if (mode == 1) rtk::k_gi_plain<1><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
     else rtk::k_gi_plain<2><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
-  } else {
+  } else if (s.layout == 1) {
     if (mode == 0) rtk::k_rs_plain<false><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
     else rtk::k_rs_plain<true><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
+  } else {
+    if (mode == 0) rtk::k_rs2_plain<false><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
+    else rtk::k_rs2_plain<true><<<grid, block, 0, stream>>>(s.words, rays, hits, n, st);
   }
   return cudaGetLastError();
 }

@@ -217,6 +217,8 @@ rt_status rt_scene_refit(rt_ctx* ctx, rt_scene* scene, uint32_t instance, const 
                          uint32_t n_positions, const uint32_t* d_indices, uint32_t n_indices, void* stream) {
   if (!ctx || !scene || !d_positions) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
   if (instance >= scene->info.instances) return fail(ctx, RT_ERR_INVALID_ARG, "no instance %u", instance);
+  if (scene->layout == RT_LAYOUT_REFLECTION_BVH2)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "refit covers the BVH4 layouts (the legacy BVH2 one is rebuilt on the host)");
   const bool gi = scene->layout == 0;
   if (!gi && !d_indices) return fail(ctx, RT_ERR_INVALID_ARG, "the reflection layout refits from the triangle list");
   std::lock_guard<std::mutex> lock(ctx->mu);

@@ -63,6 +63,8 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
 rt_status check_trace_args(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel) {
   if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null context or scene");
   if ((unsigned)mode > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown mode %d", (int)mode);
+  if (scene->layout == RT_LAYOUT_REFLECTION_BVH2 && kernel != RT_KERNEL_PLAIN)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the legacy BVH2 layout is traced by the PLAIN kernel");
   if ((unsigned)kernel > 3u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown kernel %d", (int)kernel);
   return RT_OK;
 }
@@ -152,7 +154,7 @@ rt_status rt_selftest(rt_ctx* ctx, uint32_t out[16]) {
 rt_status rt_scene_upload(rt_ctx* ctx, rt_layout layout, const uint32_t* words, size_t n_words, rt_scene** out) {
   if (!ctx || !words || !out) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
   *out = nullptr;
-  if ((unsigned)layout > 1u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown layout %d", (int)layout);
+  if ((unsigned)layout > 2u) return fail(ctx, RT_ERR_INVALID_ARG, "unknown layout %d", (int)layout);
   auto s = std::make_unique<rt_scene>();
   s->layout = (uint32_t)layout;
   std::string err;
@@ -178,7 +180,7 @@ rt_status rt_scene_upload(rt_ctx* ctx, rt_layout layout, const uint32_t* words, 
 
 rt_status rt_scene_validate(rt_layout layout, const uint32_t* words, size_t n_words, uint32_t info[8], char* err,
                             size_t err_len) {
-  if (!words || (unsigned)layout > 1u) return RT_ERR_INVALID_ARG;
+  if (!words || (unsigned)layout > 2u) return RT_ERR_INVALID_ARG;
   rtb::SceneInfo si;
   std::string e;
   bool ok = rtb::validate_scene((uint32_t)layout, words, n_words, si, e);
@@ -211,6 +213,8 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
 rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
   if (kernel != RT_KERNEL_WIDE8 && kernel != RT_KERNEL_WIDE8_PACKET) return RT_OK;  // PLAIN, FAST: the packed words
+  if (scene->layout == RT_LAYOUT_REFLECTION_BVH2)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the legacy BVH2 layout is traced by the PLAIN kernel");
   if (scene->d_wide8) return RT_OK;
   std::vector<uint32_t> words(scene->n_words);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));

@@ -274,6 +274,8 @@ rt_status rt_server_create(rt_ctx* ctx, const rt_server_desc* desc, rt_server** 
 rt_status rt_server_add_scene(rt_server* srv, rt_layout layout, const uint32_t* words, size_t n_words, uint32_t* id) {
   if (!srv || !id) return RT_ERR_INVALID_ARG;
   rt_ctx* ctx = srv->ctx;
+  if (layout == RT_LAYOUT_REFLECTION_BVH2 && srv->desc.kernel != RT_KERNEL_PLAIN)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the legacy BVH2 layout is served by a PLAIN-kernel server");
   rt_scene* scene = nullptr;
   rt_status st = rt_scene_upload(ctx, layout, words, n_words, &scene);
   if (st != RT_OK) return st;

@@ -3,6 +3,8 @@ C ABI. Integer results (hit ids, records, flags) and float results (t, barycentr
 the PLAIN and FAST kernels must be bit-identical to the oracle's."""
 from __future__ import annotations
 
+from pathlib import Path
+
 import numpy as np
 import pytest
 
@@ -310,5 +312,25 @@ def test_ray_order_is_a_permutation_and_changes_no_result(engine, key):
         got = engine.trace(scene, d, A.CLOSEST, "fast", order=order).cpu().numpy().view(np.uint32)
         want_all, _ = O.rs_trace(w, batch, False)
         check_same(got, want_all, "ordered fast")
+    finally:
+        scene.release()
+
+
+@pytest.mark.parametrize("case", ["flat", "tlas"])
+def test_legacy_bvh2_kernel_matches_the_reference_replay(engine, case):
+    """The PLAIN kernel over the legacy BVH2 layout against the golden vectors the reference's
+    own replay (tools/sunrt/replay_geometry.py) produced: t bits and hit records (barycentric
+    bits included) for closest hits; blocked flags for any hits."""
+    g = np.load(Path(__file__).resolve().parent / "golden" / "replay_bvh2.npz")
+    words, rays = g[case + "_words"], g[case + "_rays"]
+    scene = engine.upload(A.LAYOUT_REFLECTION_BVH2, words)
+    try:
+        got = gpu_trace(engine, scene, rays, A.CLOSEST, "plain").reshape(-1, 5)
+        assert np.array_equal(got[:, 0], g[case + "_closest_t"])
+        assert np.array_equal(got[:, 1:], g[case + "_closest_record"])
+        flags = gpu_trace(engine, scene, rays, A.ANY_CASTERS, "plain")
+        assert np.array_equal(flags, (g[case + "_any_record"][:, 0] != 0).astype(np.uint32))
+        with pytest.raises(A.RtError, match="UNSUPPORTED"):
+            gpu_trace(engine, scene, rays, A.CLOSEST, "fast")
     finally:
         scene.release()
