@@ -358,6 +358,62 @@ rt_status rt_pack_scene(rt_layout layout, const rt_blas* const* meshes, uint32_t
 rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);
 rt_status rt_tlas_refit(uint32_t* nodes, size_t n_words, const float* boxes, uint32_t n);
 
+/* The BLAS's positions (xyz a vertex, as given to rt_blas_build or decoded), 3 * positions floats. */
+rt_status rt_blas_positions(const rt_blas* blas, float* out);
+
+/* ---- cooked files: loading cooked scenes (far-field cuts) straight into the engine ----
+ * RLB cluster BVH (crates/asset/src/cluster_bvh/codec.rs:4-188, checked as Bvh::validate,
+ * crates/asset/src/cluster_bvh.rs:170-333) and RNF near field (crates/asset/src/near_field.rs:
+ * 540-660, NearField::validate :106-133). A rejected file returns RT_ERR_LAYOUT and, when err is
+ * not NULL, the reference's message in err (at most err_len bytes, NUL-terminated). Sizes follow
+ * the NULL-out convention: out NULL -> *n_bytes is the size; too small -> RT_ERR_INVALID_ARG. */
+#define RT_RLB_MAX_BYTES 150000000ull /* cluster_bvh::Limits::default */
+#define RT_RNF_MAX_BYTES 160000000ull /* near_field::Limits::default */
+
+/* A BLAS as an RLB file, written as the near-field builder writes its cluster BVH
+ * (near_field.rs:206-262): one zero-error level over every leaf. */
+rt_status rt_blas_encode_rlb(const rt_blas* blas, uint64_t max_bytes, uint8_t* out, size_t* n_bytes, char* err,
+                             size_t err_len);
+/* cluster_bvh::decode, then level `level`'s root over the file's records (gi_bvh.rs:62-78:
+ * Blas::new). The BLAS packs and traces as one built here. */
+rt_status rt_rlb_decode(const uint8_t* bytes, size_t n_bytes, uint64_t max_bytes, uint32_t level, rt_blas** out,
+                        char* err, size_t err_len);
+
+typedef struct rt_rnf rt_rnf;
+typedef struct rt_rnf_settings {
+  float lod_error, reach, skip;
+  uint32_t bins; /* 0, 8, 16 or 32; a mask is bins * bins / 32 words */
+} rt_rnf_settings;
+typedef struct rt_rnf_placement {
+  uint32_t mesh;
+  float transform[16];   /* column-major, the exact bits the masks were cooked under */
+  const uint32_t* masks; /* per mesh position: front side then back side, bins^2/32 words each */
+  uint64_t n_masks;
+} rt_rnf_placement;
+rt_status rt_rnf_decode(const uint8_t* bytes, size_t n_bytes, uint64_t max_bytes, rt_rnf** out, char* err,
+                        size_t err_len);
+rt_status rt_rnf_info(const rt_rnf* field, rt_rnf_settings* settings, uint8_t source[32], uint32_t* n_meshes,
+                      uint32_t* n_placements);
+/* Mesh `mesh`'s far-field cut as a BLAS (a copy: free it with rt_blas_free). */
+rt_status rt_rnf_mesh(const rt_rnf* field, uint32_t mesh, rt_blas** out);
+/* Placement k; its masks point into the field and live until rt_rnf_free. */
+rt_status rt_rnf_placement_get(const rt_rnf* field, uint32_t k, rt_rnf_placement* out);
+rt_status rt_rnf_encode(const rt_rnf_settings* settings, const uint8_t source[32], const rt_blas* const* meshes,
+                        uint32_t n_meshes, const rt_rnf_placement* placements, uint32_t n_placements,
+                        uint64_t max_bytes, uint8_t* out, size_t* n_bytes, char* err, size_t err_len);
+/* GI words for the field's meshes and the given instances (rows and the model as rt_pack_scene
+ * takes them, mesh = the field's mesh index): each mesh's placements with masks are appended
+ * after the records (gi_bvh.rs:150-227), and an instance whose model has exactly a placement's
+ * transform bits gets that placement's mask base in word 23 (gi_bvh.rs:95-104,
+ * gi_cache.rs:3225-3250); other instances get 0. */
+rt_status rt_rnf_pack_gi(const rt_rnf* field, const rt_instance* instances, uint32_t n_instances, int tlas_mode,
+                         uint32_t* out_words, size_t* n_words);
+/* A mask-free field as one world-space BLAS (gi_cache.rs:1234-1268): every placement's cut moved
+ * by its transform, mirrored windings reversed, built with RT_BUILD_SAH; bases[k] (n_placements
+ * entries) is placement k's first position. Traced as one identity instance. */
+rt_status rt_rnf_world(const rt_rnf* field, rt_blas** out, uint32_t* bases);
+void rt_rnf_free(rt_rnf* field);
+
 #ifdef __cplusplus
 }
 #endif

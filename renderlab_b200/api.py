@@ -75,6 +75,16 @@ class RtServerStats(ctypes.Structure):
                 ("wall_s", ctypes.c_double), ("device_bytes", ctypes.c_uint64), ("pending", ctypes.c_uint64)]
 
 
+class RtRnfSettings(ctypes.Structure):
+    _fields_ = [("lod_error", ctypes.c_float), ("reach", ctypes.c_float), ("skip", ctypes.c_float),
+                ("bins", ctypes.c_uint32)]
+
+
+class RtRnfPlacement(ctypes.Structure):
+    _fields_ = [("mesh", ctypes.c_uint32), ("transform", ctypes.c_float * 16),
+                ("masks", ctypes.POINTER(ctypes.c_uint32)), ("n_masks", ctypes.c_uint64)]
+
+
 class RtTuning(ctypes.Structure):
     _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
 
@@ -87,7 +97,9 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
            "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
-           "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit")
+           "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit", "rt_blas_positions",
+           "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
+           "rt_rnf_placement_get", "rt_rnf_encode", "rt_rnf_pack_gi", "rt_rnf_world", "rt_rnf_free")
 
 _lib = None
 
@@ -156,9 +168,26 @@ def lib() -> ctypes.CDLL:
                                 ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
     L.rt_tlas_build.argtypes = [_f32p, ctypes.c_uint32, ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
     L.rt_tlas_refit.argtypes = [_u32p, ctypes.c_size_t, _f32p, ctypes.c_uint32]
+    _sz = ctypes.POINTER(ctypes.c_size_t)
+    L.rt_blas_positions.argtypes = [_vp, _f32p]
+    L.rt_blas_encode_rlb.argtypes = [_vp, ctypes.c_uint64, _vp, _sz, ctypes.c_char_p, ctypes.c_size_t]
+    L.rt_rlb_decode.argtypes = [_vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(_vp),
+                                ctypes.c_char_p, ctypes.c_size_t]
+    L.rt_rnf_decode.argtypes = [_vp, ctypes.c_size_t, ctypes.c_uint64, ctypes.POINTER(_vp), ctypes.c_char_p,
+                                ctypes.c_size_t]
+    L.rt_rnf_info.argtypes = [_vp, ctypes.POINTER(RtRnfSettings), _vp, _u32p, _u32p]
+    L.rt_rnf_mesh.argtypes = [_vp, ctypes.c_uint32, ctypes.POINTER(_vp)]
+    L.rt_rnf_placement_get.argtypes = [_vp, ctypes.c_uint32, ctypes.POINTER(RtRnfPlacement)]
+    L.rt_rnf_encode.argtypes = [ctypes.POINTER(RtRnfSettings), _vp, ctypes.POINTER(_vp), ctypes.c_uint32,
+                                ctypes.POINTER(RtRnfPlacement), ctypes.c_uint32, ctypes.c_uint64, _vp, _sz,
+                                ctypes.c_char_p, ctypes.c_size_t]
+    L.rt_rnf_pack_gi.argtypes = [_vp, ctypes.POINTER(RtInstance), ctypes.c_uint32, ctypes.c_int, _u32p, _sz]
+    L.rt_rnf_world.argtypes = [_vp, ctypes.POINTER(_vp), _u32p]
+    L.rt_rnf_free.argtypes = [_vp]
+    L.rt_rnf_free.restype = None
     for name in EXPORTS:
         if name not in ("rt_ctx_destroy", "rt_blas_free", "rt_abi_version", "rt_get_last_error",
-                        "rt_scene_device_bytes"):
+                        "rt_scene_device_bytes", "rt_rnf_free"):
             getattr(L, name).restype = ctypes.c_int
     _lib = L
     return L
@@ -182,6 +211,18 @@ class Blas:
         if st != 0:
             raise RtError(st, "BVH geometry needs a nonempty, finite triangle list")
         self.h = h
+
+    @classmethod
+    def adopt(cls, h) -> "Blas":
+        """Takes ownership of a library-made BLAS handle (a decoded file's mesh); its positions
+        are the BLAS's own and its triangle list the BVH's (reordered) one."""
+        self = cls.__new__(cls)
+        self.h = h
+        info = self.info()
+        self.positions = np.zeros((info["positions"], 3), np.float32)
+        lib().rt_blas_positions(h, _np_ptr(self.positions, _f32p))
+        self.indices = self.bvh_indices()
+        return self
 
     def __del__(self):
         if getattr(self, "h", None) and _lib is not None:
@@ -211,13 +252,8 @@ class Blas:
         self.positions = p
 
 
-def pack_scene(layout: int, meshes, instances, tlas_mode: int = -1, primitives=None) -> np.ndarray:
-    """Packed words of `layout` for meshes (list of Blas) placed by `instances`.
-
-    instances: object with ``model`` (N,3,4), ``rows`` (N,3,4), ``mesh`` (N,), and optionally
-    ``casts`` (N,) bool, ``slot`` (N,), ``near_base`` (N,), ``extra`` (N,8).
-    primitives: per mesh, whether the GI layout carries its primitive table.
-    """
+def _instance_array(layout: int, instances):
+    """rt_instance records for an Instances-like object (see pack_scene)."""
     n = len(instances.mesh)
     arr = (RtInstance * max(n, 1))()
     model = np.ascontiguousarray(instances.model, np.float32).reshape(n, 12)
@@ -239,6 +275,17 @@ def pack_scene(layout: int, meshes, instances, tlas_mode: int = -1, primitives=N
                 rec.extra[k] = int(extra[i][k])
         elif casts is not None and layout == LAYOUT_GI:
             rec.extra[3] = 0 if casts[i] else 1
+    return arr, n
+
+
+def pack_scene(layout: int, meshes, instances, tlas_mode: int = -1, primitives=None) -> np.ndarray:
+    """Packed words of `layout` for meshes (list of Blas) placed by `instances`.
+
+    instances: object with ``model`` (N,3,4), ``rows`` (N,3,4), ``mesh`` (N,), and optionally
+    ``casts`` (N,) bool, ``slot`` (N,), ``near_base`` (N,), ``extra`` (N,8).
+    primitives: per mesh, whether the GI layout carries its primitive table.
+    """
+    arr, n = _instance_array(layout, instances)
     m = len(meshes)
     handles = (_vp * max(m, 1))(*[b.h for b in meshes])
     pos_ptrs = (_f32p * max(m, 1))(*[_np_ptr(b.positions, _f32p) for b in meshes])

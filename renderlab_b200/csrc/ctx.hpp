@@ -41,6 +41,10 @@ struct rt_blas {
   rtb::Blas b;
 };
 
+struct rt_rnf {
+  rtb::Rnf f;
+};
+
 struct rt_ctx {
   int device = 0;
   rtk::DevStatus* d_status = nullptr;

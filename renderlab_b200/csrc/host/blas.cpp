@@ -185,6 +185,7 @@ class Builder {
     uint32_t id = (uint32_t)out_->leaf_count();
     out_->leaves.push_back(offset);
     out_->leaves.push_back((uint32_t)(3 * (hi - lo)));
+    out_->leaf_source.push_back((uint32_t)(3 * (size_t)perm_[lo]));  // Leaf::source_index_offset
     return id | LEAF;
   }
 

@@ -44,6 +44,7 @@ struct Blas {
   std::vector<uint32_t> leaves;   // (index offset, index count) a leaf
   std::vector<float> positions;   // xyz a vertex (the input positions, unchanged)
   std::vector<uint32_t> indices;  // reordered triangle list
+  std::vector<uint32_t> leaf_source;  // per leaf: 3 * its first triangle's index in the source list
   uint32_t root = EMPTY;
   Aabb bounds;                    // every position (gi_bvh.rs:70)
   size_t node_count() const { return nodes.size() / 16; }
@@ -70,17 +71,55 @@ struct Placement {
   uint32_t mesh, slot, casts_shadow, near_base;
   uint32_t extra[8];
 };
+// One cooked placement's near-field masks (gi_bvh.rs:38-43): the column-major transform they
+// were cooked under and two sides of bins^2/32 words per BLAS position.
+struct NearMasks {
+  float transform[16];
+  const uint32_t* masks;
+  size_t n_masks;
+};
 struct MeshRef {
   const Blas* blas;
   const float* positions;  // source positions (reflection triangles are written from them)
   const uint32_t* indices; // source triangle list (primitive ids)
   size_t n_indices;
   bool primitives;         // GI: append the primitive table
+  // GI: masks appended after every mesh's records (gi_bvh.rs:150-178); an instance of this mesh
+  // whose model has exactly one entry's transform bits gets that entry's base in word 23.
+  std::vector<NearMasks> near = {};
 };
 bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst, int tlas_mode,
              std::vector<uint32_t>& out, std::string& err);
 bool pack_reflection(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst,
                      int tlas_mode, std::vector<uint32_t>& out, std::string& err);
+
+// Cooked files (cooked.cpp). RLB: crates/asset/src/cluster_bvh/codec.rs; RNF:
+// crates/asset/src/near_field.rs:540-660. A BLAS is written as the near-field builder's cluster
+// BVH (one zero-error level over every leaf); decoding one level gives a BLAS. max_bytes is the
+// reference's Limits::max_bytes (160,000,000 by default, near_field.rs:86-92).
+struct RnfSettings {
+  float lod_error = 0.0f, reach = 0.0f, skip = 0.0f;
+  uint32_t bins = 0;
+};
+struct RnfPlacement {
+  uint32_t mesh = 0;
+  float transform[16] = {};  // four columns of four
+  std::vector<uint32_t> masks;
+};
+struct Rnf {
+  RnfSettings settings;
+  uint8_t source[32] = {};
+  std::vector<Blas> meshes;
+  std::vector<RnfPlacement> placements;
+};
+bool encode_rlb(const Blas& b, uint64_t max_bytes, std::vector<uint8_t>& out, std::string& err);
+bool decode_rlb(const uint8_t* bytes, size_t n, uint64_t max_bytes, uint32_t level, Blas& out, std::string& err);
+bool encode_rnf(const Rnf& f, uint64_t max_bytes, std::vector<uint8_t>& out, std::string& err);
+bool decode_rnf(const uint8_t* bytes, size_t n, uint64_t max_bytes, Rnf& out, std::string& err);
+// World::new (src/gi_cache.rs:1234-1268): every placement's cut moved to world space (winding
+// reversed under a mirroring transform) and built as one SAH BLAS; bases[k] is placement k's
+// first position in it.
+bool rnf_world(const Rnf& f, Blas& out, std::vector<uint32_t>& bases, std::string& err);
 
 // What a validated buffer holds, for the launchers and the derived layouts.
 struct SceneInfo {

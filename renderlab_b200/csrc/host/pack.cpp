@@ -85,6 +85,19 @@ void world_box(const float* model, const Aabb& obj, Aabb& out) {
   }
 }
 
+// Blas::near_base (gi_bvh.rs:95-104): the base of the first masks cooked under exactly this
+// model's bits (an affine model: the column-major transform's last row is 0, 0, 0, 1), else 0.
+uint32_t near_base(const float* model, const std::vector<NearMasks>& near, const std::vector<size_t>& bases) {
+  for (size_t k = 0; k < near.size(); ++k) {
+    const float* t = near[k].transform;
+    bool same = as_bits(t[3]) == 0 && as_bits(t[7]) == 0 && as_bits(t[11]) == 0 && as_bits(t[15]) == as_bits(1.0f);
+    for (int r = 0; r < 3; ++r)
+      for (int c = 0; c < 4; ++c) same = same && as_bits(model[4 * r + c]) == as_bits(t[4 * c + r]);
+    if (same) return (uint32_t)bases[k];
+  }
+  return 0;
+}
+
 }  // namespace
 
 bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst, int tlas_mode,
@@ -102,6 +115,13 @@ bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& i
     base[m][3] = base[m][2] + (uint32_t)b.positions.size();
     at = base[m][3] + b.indices.size() + prims[m].size();
   }
+  // gi_bvh.rs:165-177: every mesh's near-field masks after all the records, mesh by mesh.
+  std::vector<std::vector<size_t>> near(meshes.size());
+  for (size_t m = 0; m < meshes.size(); ++m)
+    for (const NearMasks& q : meshes[m].near) {
+      near[m].push_back(at);
+      at += q.n_masks;
+    }
   if (at >= (size_t)UINT32_MAX) {
     err = "packed GI geometry exceeds 2^32 words";
     return false;
@@ -130,7 +150,7 @@ bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& i
     }
     for (int k = 0; k < 4; ++k) r[18 + k] = base[g.mesh][k];
     r[22] = b.root;
-    r[23] = g.near_base;
+    r[23] = meshes[g.mesh].near.empty() ? g.near_base : near_base(g.model, meshes[g.mesh].near, near[g.mesh]);
     for (int k = 0; k < 8; ++k) r[24 + k] = g.extra[k];
     r[28] = prims[g.mesh].empty() ? 0u : base[g.mesh][3] + (uint32_t)b.indices.size();
   }
@@ -146,6 +166,8 @@ bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& i
     for (size_t k = 0; k < b.positions.size(); ++k) p[k] = as_bits(b.positions[k]);
     std::copy(b.indices.begin(), b.indices.end(), out.data() + base[m][3]);
     std::copy(prims[m].begin(), prims[m].end(), out.data() + base[m][3] + b.indices.size());
+    for (size_t k = 0; k < meshes[m].near.size(); ++k)
+      std::copy(meshes[m].near[k].masks, meshes[m].near[k].masks + meshes[m].near[k].n_masks, out.data() + near[m][k]);
   }
   return true;
 }

@@ -536,3 +536,180 @@ rt_status rt_trace_gi_cells(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, co
   ctx->launches += 1;
   return RT_OK;
 }
+
+// ---------------------------------------------------------------- cooked files
+
+namespace {
+
+rt_status cooked_error(const std::string& what, char* err, size_t err_len) {
+  if (err && err_len) {
+    const size_t k = std::min(what.size(), err_len - 1);
+    std::memcpy(err, what.data(), k);
+    err[k] = 0;
+  }
+  return RT_ERR_LAYOUT;
+}
+
+rt_status copy_out(const std::vector<uint8_t>& bytes, uint8_t* out, size_t* n_bytes) {
+  if (!out) {
+    *n_bytes = bytes.size();
+    return RT_OK;
+  }
+  const bool fits = *n_bytes >= bytes.size();
+  *n_bytes = bytes.size();
+  if (!fits) return RT_ERR_INVALID_ARG;
+  std::copy(bytes.begin(), bytes.end(), out);
+  return RT_OK;
+}
+
+}  // namespace
+
+rt_status rt_blas_positions(const rt_blas* blas, float* out) {
+  if (!blas || !out) return RT_ERR_INVALID_ARG;
+  std::copy(blas->b.positions.begin(), blas->b.positions.end(), out);
+  return RT_OK;
+}
+
+rt_status rt_blas_encode_rlb(const rt_blas* blas, uint64_t max_bytes, uint8_t* out, size_t* n_bytes, char* err,
+                             size_t err_len) {
+  if (!blas || !n_bytes) return RT_ERR_INVALID_ARG;
+  std::vector<uint8_t> bytes;
+  std::string why;
+  if (!rtb::encode_rlb(blas->b, max_bytes, bytes, why)) return cooked_error(why, err, err_len);
+  return copy_out(bytes, out, n_bytes);
+}
+
+rt_status rt_rlb_decode(const uint8_t* bytes, size_t n_bytes, uint64_t max_bytes, uint32_t level, rt_blas** out,
+                        char* err, size_t err_len) {
+  if ((!bytes && n_bytes) || !out) return RT_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto b = std::make_unique<rt_blas>();
+  std::string why;
+  if (!rtb::decode_rlb(bytes, n_bytes, max_bytes, level, b->b, why)) return cooked_error(why, err, err_len);
+  *out = b.release();
+  return RT_OK;
+}
+
+rt_status rt_rnf_decode(const uint8_t* bytes, size_t n_bytes, uint64_t max_bytes, rt_rnf** out, char* err,
+                        size_t err_len) {
+  if ((!bytes && n_bytes) || !out) return RT_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto f = std::make_unique<rt_rnf>();
+  std::string why;
+  static const uint8_t none[1] = {0};
+  if (!rtb::decode_rnf(bytes ? bytes : none, n_bytes, max_bytes, f->f, why)) return cooked_error(why, err, err_len);
+  *out = f.release();
+  return RT_OK;
+}
+
+rt_status rt_rnf_info(const rt_rnf* field, rt_rnf_settings* settings, uint8_t source[32], uint32_t* n_meshes,
+                      uint32_t* n_placements) {
+  if (!field) return RT_ERR_INVALID_ARG;
+  const rtb::Rnf& f = field->f;
+  if (settings) *settings = rt_rnf_settings{f.settings.lod_error, f.settings.reach, f.settings.skip, f.settings.bins};
+  if (source) std::memcpy(source, f.source, 32);
+  if (n_meshes) *n_meshes = (uint32_t)f.meshes.size();
+  if (n_placements) *n_placements = (uint32_t)f.placements.size();
+  return RT_OK;
+}
+
+rt_status rt_rnf_mesh(const rt_rnf* field, uint32_t mesh, rt_blas** out) {
+  if (!field || !out || mesh >= field->f.meshes.size()) return RT_ERR_INVALID_ARG;
+  auto b = std::make_unique<rt_blas>();
+  b->b = field->f.meshes[mesh];
+  *out = b.release();
+  return RT_OK;
+}
+
+rt_status rt_rnf_placement_get(const rt_rnf* field, uint32_t k, rt_rnf_placement* out) {
+  if (!field || !out || k >= field->f.placements.size()) return RT_ERR_INVALID_ARG;
+  const rtb::RnfPlacement& p = field->f.placements[k];
+  out->mesh = p.mesh;
+  std::copy(p.transform, p.transform + 16, out->transform);
+  out->masks = p.masks.data();
+  out->n_masks = p.masks.size();
+  return RT_OK;
+}
+
+rt_status rt_rnf_encode(const rt_rnf_settings* settings, const uint8_t source[32], const rt_blas* const* meshes,
+                        uint32_t n_meshes, const rt_rnf_placement* placements, uint32_t n_placements,
+                        uint64_t max_bytes, uint8_t* out, size_t* n_bytes, char* err, size_t err_len) {
+  if (!settings || !source || !n_bytes || (n_meshes && !meshes) || (n_placements && !placements))
+    return RT_ERR_INVALID_ARG;
+  rtb::Rnf f;
+  f.settings = rtb::RnfSettings{settings->lod_error, settings->reach, settings->skip, settings->bins};
+  std::memcpy(f.source, source, 32);
+  for (uint32_t m = 0; m < n_meshes; ++m) {
+    if (!meshes[m]) return RT_ERR_INVALID_ARG;
+    f.meshes.push_back(meshes[m]->b);
+  }
+  for (uint32_t k = 0; k < n_placements; ++k) {
+    const rt_rnf_placement& s = placements[k];
+    if (s.n_masks && !s.masks) return RT_ERR_INVALID_ARG;
+    rtb::RnfPlacement p;
+    p.mesh = s.mesh;
+    std::copy(s.transform, s.transform + 16, p.transform);
+    p.masks.assign(s.masks, s.masks + s.n_masks);
+    f.placements.push_back(std::move(p));
+  }
+  std::vector<uint8_t> bytes;
+  std::string why;
+  if (!rtb::encode_rnf(f, max_bytes, bytes, why)) return cooked_error(why, err, err_len);
+  return copy_out(bytes, out, n_bytes);
+}
+
+rt_status rt_rnf_pack_gi(const rt_rnf* field, const rt_instance* instances, uint32_t n_instances, int tlas_mode,
+                         uint32_t* out_words, size_t* n_words) {
+  if (!field || !n_words || (n_instances && !instances)) return RT_ERR_INVALID_ARG;
+  const rtb::Rnf& f = field->f;
+  std::vector<rtb::MeshRef> refs(f.meshes.size());
+  for (size_t m = 0; m < f.meshes.size(); ++m) {
+    const rtb::Blas& b = f.meshes[m];
+    refs[m] = rtb::MeshRef{&b, b.positions.data(), b.indices.data(), b.indices.size(), false};
+  }
+  // set_indirect_near_field (gi_cache.rs:3240-3248): per mesh, its placements that have masks.
+  for (const rtb::RnfPlacement& p : f.placements) {
+    if (p.masks.empty()) continue;
+    rtb::NearMasks q;
+    std::copy(p.transform, p.transform + 16, q.transform);
+    q.masks = p.masks.data(), q.n_masks = p.masks.size();
+    refs[p.mesh].near.push_back(q);
+  }
+  std::vector<rtb::Placement> inst(n_instances);
+  for (uint32_t i = 0; i < n_instances; ++i) {
+    const rt_instance& s = instances[i];
+    rtb::Placement& p = inst[i];
+    std::copy(s.model, s.model + 12, p.model);
+    std::copy(s.rows, s.rows + 12, p.rows);
+    p.mesh = s.mesh, p.slot = s.slot, p.casts_shadow = s.casts_shadow, p.near_base = 0;
+    std::copy(s.extra, s.extra + 8, p.extra);
+  }
+  std::vector<uint32_t> words;
+  std::string err;
+  if (!rtb::pack_gi(refs, inst, tlas_mode, words, err)) return RT_ERR_LAYOUT;
+  if (!out_words) {
+    *n_words = words.size();
+    return RT_OK;
+  }
+  if (*n_words < words.size()) {
+    *n_words = words.size();
+    return RT_ERR_INVALID_ARG;
+  }
+  std::copy(words.begin(), words.end(), out_words);
+  *n_words = words.size();
+  return RT_OK;
+}
+
+rt_status rt_rnf_world(const rt_rnf* field, rt_blas** out, uint32_t* bases) {
+  if (!field || !out) return RT_ERR_INVALID_ARG;
+  *out = nullptr;
+  auto b = std::make_unique<rt_blas>();
+  std::vector<uint32_t> at;
+  std::string err;
+  if (!rtb::rnf_world(field->f, b->b, at, err)) return RT_ERR_INVALID_ARG;
+  if (bases) std::copy(at.begin(), at.end(), bases);
+  *out = b.release();
+  return RT_OK;
+}
+
+void rt_rnf_free(rt_rnf* field) { delete field; }
