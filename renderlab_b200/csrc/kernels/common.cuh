@@ -57,6 +57,14 @@ RT_DEV F3 ld3(const uint32_t* __restrict__ w, size_t i) { return {ldf(w, i), ldf
 RT_DEV uint4 ld4(const uint32_t* __restrict__ w, size_t i) {
   return __ldg(reinterpret_cast<const uint4*>(w + i));
 }
+// Four words at any word offset: one 16-byte load when the offset is a multiple of 4, else four
+// word loads. The reference's packers align only some records: GI meshes follow one another
+// with no padding, so a mesh's node records start wherever the previous mesh ended. The offset's
+// alignment is the same for every node of a mesh, so lanes of one mesh take the same path.
+RT_DEV uint4 ld4u(const uint32_t* __restrict__ w, size_t i) {
+  if ((i & 3) == 0) return __ldg(reinterpret_cast<const uint4*>(w + i));
+  return make_uint4(__ldg(w + i), __ldg(w + i + 1), __ldg(w + i + 2), __ldg(w + i + 3));
+}
 
 struct Ray {
   F3 o;

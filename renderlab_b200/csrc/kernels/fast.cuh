@@ -117,7 +117,7 @@ RT_DEV bool rs_leaf(const uint32_t* __restrict__ w, RsLane<AM>& L, uint32_t chil
   const F3 o = L.o, d = L.d;
   for (uint32_t k = 0; k < count; ++k) {
     const size_t X = L.tris + (size_t)(start + k) * 12;
-    const uint4 w0 = ld4(w, X), w1 = ld4(w, X + 4), w2 = ld4(w, X + 8);
+    const uint4 w0 = ld4u(w, X), w1 = ld4u(w, X + 4), w2 = ld4u(w, X + 8);
     const F3 a = {__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
     const F3 e1 = {__uint_as_float(w0.w), __uint_as_float(w1.x), __uint_as_float(w1.y)};
     const F3 e2 = {__uint_as_float(w1.z), __uint_as_float(w1.w), __uint_as_float(w2.x)};
@@ -149,7 +149,7 @@ RT_DEV bool rs_leaf(const uint32_t* __restrict__ w, RsLane<AM>& L, uint32_t chil
 template <int AM>
 RT_DEV void rs_node(const uint32_t* __restrict__ w, RsLane<AM>& L, uint32_t child, uint32_t* stack, DevStatus* st) {
   const size_t N = L.nodes + (size_t)child * 16;
-  const uint4 n0 = ld4(w, N), n1 = ld4(w, N + 4), n2 = ld4(w, N + 8), n3 = ld4(w, N + 12);
+  const uint4 n0 = ld4u(w, N), n1 = ld4u(w, N + 4), n2 = ld4u(w, N + 8), n3 = ld4u(w, N + 12);
   const float lim = rs_limit(L.best, L.inst);
   const F3 base = {__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z)};
   const F3 step = {__uint_as_float(n0.w), __uint_as_float(n1.x), __uint_as_float(n1.y)};
@@ -374,7 +374,7 @@ RT_DEV bool gi_leaf(const uint32_t* __restrict__ w, GiLane<AM>& L, uint32_t chil
 template <int AM>
 RT_DEV void gi_node(const uint32_t* __restrict__ w, GiLane<AM>& L, uint32_t child, uint32_t* stack, DevStatus* st) {
   const size_t n = L.nodes + (size_t)child * 16;
-  const uint4 n0 = ld4(w, n), n1 = ld4(w, n + 4), n2 = ld4(w, n + 8), n3 = ld4(w, n + 12);
+  const uint4 n0 = ld4u(w, n), n1 = ld4u(w, n + 4), n2 = ld4u(w, n + 8), n3 = ld4u(w, n + 12);
   const F3 oq = {__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z)};
   const F3 step = {__uint_as_float(n0.w), __uint_as_float(n1.x), __uint_as_float(n1.y)};
   uint32_t c[4] = {n1.z, n1.w, n2.x, n2.y};

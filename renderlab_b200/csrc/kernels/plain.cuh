@@ -272,7 +272,7 @@ RT_DEV bool rs_instance(const uint32_t* __restrict__ w, uint32_t i, const Ray& r
         const uint32_t start = (child & ~LEAF) >> 4;
         for (uint32_t k = 0; k < (child & 15u); ++k) {
           const size_t X = tris + (size_t)(start + k) * 12;
-          const uint4 w0 = ld4(w, X), w1 = ld4(w, X + 4), w2 = ld4(w, X + 8);
+          const uint4 w0 = ld4u(w, X), w1 = ld4u(w, X + 4), w2 = ld4u(w, X + 8);
           const F3 a = {__uint_as_float(w0.x), __uint_as_float(w0.y), __uint_as_float(w0.z)};
           const F3 e1 = {__uint_as_float(w0.w), __uint_as_float(w1.x), __uint_as_float(w1.y)};
           const F3 e2 = {__uint_as_float(w1.z), __uint_as_float(w1.w), __uint_as_float(w2.x)};
@@ -298,7 +298,7 @@ RT_DEV bool rs_instance(const uint32_t* __restrict__ w, uint32_t i, const Ray& r
         break;
       }
       const size_t N = nodes + (size_t)child * 16;
-      const uint4 n0 = ld4(w, N), n1 = ld4(w, N + 4), n2 = ld4(w, N + 8), n3 = ld4(w, N + 12);
+      const uint4 n0 = ld4u(w, N), n1 = ld4u(w, N + 4), n2 = ld4u(w, N + 8), n3 = ld4u(w, N + 12);
       const float lim = rs_limit(best, i);
       const F3 base = {__uint_as_float(n0.x), __uint_as_float(n0.y), __uint_as_float(n0.z)};
       const F3 step = {__uint_as_float(n0.w), __uint_as_float(n1.x), __uint_as_float(n1.y)};

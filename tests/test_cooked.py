@@ -7,6 +7,7 @@ import struct
 import numpy as np
 import pytest
 
+from oracle import oracle as O
 from renderlab_b200 import api as A
 from renderlab_b200 import cooked as C
 from renderlab_b200.scenes import Instances
@@ -358,30 +359,43 @@ def test_rnf_world_merges_placements_in_world_space():
 
 @pytest.mark.gpu
 def test_cooked_field_traces_as_the_built_meshes():
-    """A decoded field's GI words trace exactly as the same meshes packed from the builder: the
-    masks change word 23 and the tail, never what a ray hits."""
+    """A decoded field's GI words trace exactly as the same meshes packed from the builder (the
+    masks change word 23 and the tail, never what a ray hits), and PLAIN gives the oracle's hits."""
     import torch
-    from renderlab_b200.scenes import Stream
     f = field_of(placements=6)
     g = C.NearField.decode(f.encode())
     inst = f.instances()
+    words = g.pack_gi(inst)
+    # The second mesh's node records start off a 16-byte boundary (GI meshes are not padded):
+    # the FAST kernel's node loads must not assume alignment.
+    assert words[16 + 32 + 18] % 4 != 0
     eng = A.Engine(0)
     try:
-        a = eng.upload(A.LAYOUT_GI, g.pack_gi(inst))
+        a = eng.upload(A.LAYOUT_GI, words)
         b = eng.upload(A.LAYOUT_GI, A.pack_scene(A.LAYOUT_GI, f.meshes, inst))
-        s = Stream(5)
+        # rays aimed at the placements' vertices from above (about 30 % hit)
+        rng = np.random.default_rng(5)
         n = 1 << 14
-        o = s.range(-2, 20, n, 3).astype(np.float32)
-        o[:, 1] = 3.0
-        d = s.unit_vectors(n).astype(np.float32)
-        d[:, 1] = -np.abs(d[:, 1]) - 0.2
-        d /= np.linalg.norm(d, axis=1, keepdims=True)
+        pts = np.concatenate([f.meshes[p.mesh].positions @ p.transform[:3, :3] + p.transform[3, :3]
+                              for p in f.placements])
+        tgt = pts[rng.integers(0, len(pts), n)] + rng.normal(0, 0.05, (n, 3))
+        o = tgt + np.array([0.0, 3.0, 0.0]) + rng.normal(0, 0.5, (n, 3))
+        d = (tgt - o) / np.linalg.norm(tgt - o, axis=1, keepdims=True)
         rays = np.concatenate([o, np.zeros((n, 1)), d, np.full((n, 1), 1e4)], 1).astype(np.float32)
         r = torch.from_numpy(rays).cuda()
+        a.prepare("wide8")
+        b.prepare("wide8")
+        plain = None
         for kernel in ("plain", "fast", "wide8"):
-            ha = eng.trace(a, r, A.CLOSEST, kernel).cpu().numpy()
-            hb = eng.trace(b, r, A.CLOSEST, kernel).cpu().numpy()
-            assert (ha.view(np.uint32) == hb.view(np.uint32)).all(), kernel
+            ha = eng.trace(a, r, A.CLOSEST, kernel).cpu().numpy().view(np.uint32)
+            hb = eng.trace(b, r, A.CLOSEST, kernel).cpu().numpy().view(np.uint32)
+            assert (ha == hb).all(), kernel
+            if kernel == "plain":
+                plain = ha
+                assert (plain[:, 1] != A.MISS).mean() > 0.2  # the rays do hit the field
+                assert (plain == O.gi_trace(words, rays, 0)[0]).all()  # the oracle's hits, bit for bit
+            elif kernel == "fast":
+                assert (ha == plain).all()  # FAST is bit-identical to PLAIN
         torch.cuda.synchronize()
         a.release()
         b.release()
