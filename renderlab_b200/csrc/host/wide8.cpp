@@ -214,7 +214,10 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
     uint8_t meta[8] = {}, q[6][8] = {};
     uint32_t inner = 0, offset = 0;
     for (int s = 0; s < 8; ++s) {
-      if (slot_of[s] < 0) continue;
+      if (slot_of[s] < 0) {  // empty: an inverted box (lower 255, upper 0) that no ray meets
+        for (int a = 0; a < 3; ++a) q[a][s] = 255, q[3 + a][s] = 0;
+        continue;
+      }
       const BNode& k = bn[kids[slot_of[s]]];
       for (int a = 0; a < 3; ++a) {
         const double sc = std::ldexp(1.0, ex[a]);

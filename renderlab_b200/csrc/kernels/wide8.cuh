@@ -24,6 +24,10 @@ constexpr float W8_U = 5.9604645e-8f;  // 2^-24
 constexpr float W8_TIE = 8e-6f;
 constexpr float W8_EDGE = 1e-5f;
 constexpr uint32_t W8_STACK = 32;
+// Resident 128-thread blocks per SM the register allocation is sized for (4: 128 registers).
+#ifndef RT_W8_MIN_BLOCKS
+#define RT_W8_MIN_BLOCKS 4
+#endif
 
 // Opt-in device counters of the WIDE8 walk (diagnostics and the bytes-per-ray roofline).
 enum W8Count { W8C_RAYS, W8C_TOP_NODES, W8C_INSTANCE_TESTS, W8C_NODES, W8C_LEAVES, W8C_TRIS, W8C_RETESTS, W8C_FINAL64, W8C_N };
@@ -305,11 +309,13 @@ RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, co
               Bz = __fmul_rn(__fsub_rn(pz, R.o.z), R.inv.z);
   // Per axis, |error of a plane's t| <= u (2 * 255 * 2^-15 |A'| + 3 |B|) (the rounding of 1/d,
   // of 2^e / d, of p - o and of (p - o) / d) + 2 u (|B| + |A'|) (the rounding of B - A' and of
-  // C -/+ E) + u |t| (the fma). The absolute part, doubled, moves the near planes down and the far
-  // planes up; the relative part is applied to the entry / exit after the max / min.
-  const float Ex = 2.0f * W8_U * fmaf(2.1f, fabsf(Ax), 6.0f * fabsf(Bx));
-  const float Ey = 2.0f * W8_U * fmaf(2.1f, fabsf(Ay), 6.0f * fabsf(By));
-  const float Ez = 2.0f * W8_U * fmaf(2.1f, fabsf(Az), 6.0f * fabsf(Bz));
+  // C -/+ E) + u |t| (the fma), and |t| <= (1 + 255 * 2^-15) |A'| + |C| + |E| <= 2.01 |A'| + 1.01 |B|.
+  // So each plane is within u (4.02 |A'| + 6.01 |B|) of exact; doubled (8.4 |A'| + 14.2 |B| with
+  // margin for E's own rounding) it moves the near planes down and the far planes up. The max /
+  // min of the planes adds no rounding, so the entry and exit need no further widening.
+  const float Ex = 2.0f * W8_U * fmaf(4.2f, fabsf(Ax), 7.1f * fabsf(Bx));
+  const float Ey = 2.0f * W8_U * fmaf(4.2f, fabsf(Ay), 7.1f * fabsf(By));
+  const float Ez = 2.0f * W8_U * fmaf(4.2f, fabsf(Az), 7.1f * fabsf(Bz));
   const float Cx = __fsub_rn(Bx, Ax), Cy = __fsub_rn(By, Ay), Cz = __fsub_rn(Bz, Az);
   const float Bnx = Cx - Ex, Bfx = Cx + Ex, Bny = Cy - Ey, Bfy = Cy + Ey, Bnz = Cz - Ez, Bfz = Cz + Ez;
   // near / far planes per axis by the direction's sign
@@ -326,19 +332,10 @@ RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, co
     const float tnx = fmaf(q15(s < 4 ? nx0 : nx1, b), Ax, Bnx), tfx = fmaf(q15(s < 4 ? fx0 : fx1, b), Ax, Bfx);
     const float tny = fmaf(q15(s < 4 ? ny0 : ny1, b), Ay, Bny), tfy = fmaf(q15(s < 4 ? fy0 : fy1, b), Ay, Bfy);
     const float tnz = fmaf(q15(s < 4 ? nz0 : nz1, b), Az, Bnz), tfz = fmaf(q15(s < 4 ? fz0 : fz1, b), Az, Bfz);
-    float tn = fmaxf(fmaxf(tnx, tny), tnz), tf = fminf(fminf(tfx, tfy), tfz);
-    tn = fmaf(-2.0f * W8_U, fabsf(tn), tn);
-    tf = fmaf(2.0f * W8_U, fabsf(tf), tf);
-    if (fmaxf(tn, tmin) <= fminf(tf, lim)) hits |= 1u << s;
+    const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin)), tf = fminf(fminf(tfx, tfy), fminf(tfz, lim));
+    if (tn <= tf) hits |= 1u << s;
   }
   return hits;
-}
-
-// A slot is a leaf when its meta byte has a count; empty slots have neither.
-RT_DEV uint32_t w8_leafmask(uint32_t meta_lo, uint32_t meta_hi) {
-  return ((meta_lo & 0xe0u) ? 1u : 0u) | ((meta_lo & 0xe000u) ? 2u : 0u) | ((meta_lo & 0xe00000u) ? 4u : 0u) |
-         ((meta_lo & 0xe0000000u) ? 8u : 0u) | ((meta_hi & 0xe0u) ? 16u : 0u) | ((meta_hi & 0xe000u) ? 32u : 0u) |
-         ((meta_hi & 0xe00000u) ? 64u : 0u) | ((meta_hi & 0xe0000000u) ? 128u : 0u);
 }
 
 // One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
@@ -355,7 +352,9 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const W8Best& best = L.best;
   const float lim = best.hit ? best.t + 2.0f * best.band + W8_TIE * best.t : L.ray.tmax;
   const uint32_t hits = w8_box_hits(R, a0, a2, a3, a4, L.ray.tmin, lim);
-  uint32_t leaf_hits = hits & w8_leafmask(meta_lo, meta_hi);
+  // Empty slots hold inverted boxes, which no ray meets; one that is met all the same (a node
+  // tiny beside its distance, where the widening exceeds 255 steps) has a zero count.
+  uint32_t leaf_hits = hits & ~imask;
   while (leaf_hits) {
     const uint32_t s = __ffs(leaf_hits) - 1;
     leaf_hits &= leaf_hits - 1;
@@ -481,7 +480,7 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
 // step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
 // re-converges at the top of the loop.
 template <uint32_t LAYOUT, int AM, int BLOCK, bool COUNT, class Src>
-__global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__ w, W8View V, const Src src,
+__global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                  unsigned int* __restrict__ counter, uint32_t n, DevStatus* st,
                                                  unsigned long long* cnt, uint32_t refill) {
   uint2 stack[W8_STACK];
@@ -565,7 +564,7 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8(const uint32_t* __restrict__
 // depend on the visit order (conservative boxes, ties resolved in f64 on (t, instance,
 // triangle)), so each ray gets the hit the per-ray walk finds.
 template <uint32_t LAYOUT, int AM, int BLOCK, class Src>
-__global__ void __launch_bounds__(BLOCK, 4) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
+__global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                            unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
   __shared__ uint2 warp_stack[BLOCK / 32][W8_STACK];
   uint2* stack = warp_stack[threadIdx.x >> 5];
@@ -616,7 +615,7 @@ __global__ void __launch_bounds__(BLOCK, 4) k_wide8_packet(const uint32_t* __res
           hits = w8_box_hits(L.R, a0, a2, a3, a4, L.ray.tmin, lim);
         }
         // leaves: every lane whose ray meets one tests its triangles
-        for (uint32_t lh = __reduce_or_sync(0xffffffffu, hits & w8_leafmask(meta_lo, meta_hi)); lh; lh &= lh - 1) {
+        for (uint32_t lh = __reduce_or_sync(0xffffffffu, hits & ~imask); lh; lh &= lh - 1) {
           const uint32_t s = __ffs(lh) - 1;
           if (!in || !(hits >> s & 1u)) continue;
           const uint32_t m = ((s < 4 ? meta_lo : meta_hi) >> (8 * (s & 3))) & 0xffu;
