@@ -1,5 +1,5 @@
 // Builder of the compressed 8-wide BLAS (layout in wide8.hpp): a binned-SAH binary tree with
-// leaves of at most three triangles, collapsed top-down into 8-wide nodes by repeatedly opening
+// leaves of at most W8_MAX_LEAF triangles, collapsed top-down into 8-wide nodes by repeatedly opening
 // the child of largest surface area, child slots assigned by octant, child boxes quantised
 // outward to 8 bits against a power-of-two scale.
 #include "wide8.hpp"
