@@ -274,6 +274,14 @@ def wide8_bytes(counters, layout, hit_bytes):
         + 48 * c["triangles"]
 
 
+# DRAM bytes per ray (read + write) that ncu measured on a launch, by (config, --small, kernel);
+# the capture command and figures are in profiles/k_wide8_clusters250k_gi.md. The capture is the
+# reduced clusters case (250k triangles, 1M GI rays); the full case reuses its bytes per ray,
+# since a ray's compulsory traffic is its own ray and hit plus its share of one scene read
+# (about 17 bytes a ray in both).
+TRAFFIC = {(2, True, "k_wide8"): 67.8, (2, False, "k_wide8"): 67.8}
+
+
 def hit_bytes(layout, mode):
     return 4 if mode else (40 if layout == 0 else 20)
 
@@ -726,28 +734,48 @@ def run_ours(args):
         cpu, counts = cpu_baseline_leg(wl, args.cpu_seconds)
     peak, peak_kind = measured_peak()
     roof = None
-    alg = 0.0
     notes = []
+    # Algorithmic bytes of each group's launch: the 8-wide walk's visit counters (every 16th ray)
+    # for WIDE8 and its packet walk (which serves the same per-ray walks), else the oracle's BVH4
+    # counters on its CPU sample.
+    group_bytes = []
     for g, p in zip(wl.groups, plans):
         kern = p.desc["kernel"] if p is not None else "plain"
+        gb = 0.0
         for i in g:
             b = wl.batches[i]
             hb = hit_bytes(wl.layout, b.mode)
-            if kern == "wide8":  # the 8-wide walk's visit counters on every 16th ray
+            if kern in ("wide8", "wide8p"):
                 c = engine.trace_counted(scene, dev[i][::16].contiguous(), b.mode, "wide8")
-                alg += wide8_bytes(c, wl.layout, hb) * len(b.rays) / max(1, c["rays"])
+                gb += wide8_bytes(c, wl.layout, hb) * len(b.rays) / max(1, c["rays"])
             elif counts is not None:
                 cnt, nsamp = counts
-                alg += bvh4_bytes(cnt[i], nsamp[i], wl.layout, hb) * len(b.rays) / max(1, nsamp[i])
+                gb += bvh4_bytes(cnt[i], nsamp[i], wl.layout, hb) * len(b.rays) / max(1, nsamp[i])
             else:
+                gb = None
                 notes.append("no oracle counters (--no-cpu): BVH4 bytes not counted")
-    if alg > 0:
-        achieved = alg / (ms * 1e-3) / 1e9
-        roof = dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak, traffic=None,
-                    peak_source=f"{peak_kind} hbm_gbs", bytes_per_ray=alg / n_step,
-                    roofline_mrays=peak * 1e9 / (alg / n_step) / 1e6,
-                    note="algorithmic bytes of the chosen kernels' walks (visit counters) over the product time; "
-                         "scenes under 126 MB are L2-resident, so the HBM fraction is a ceiling check, not the limit")
+                break
+        group_bytes.append(gb)
+    group_ms = prod_ms.mean(0)
+    dom = int(np.argmax(group_ms))
+    if group_bytes[dom]:
+        p = plans[dom]
+        kern = p.desc["kernel"] if p is not None else "plain"
+        name = {"wide8": "k_wide8", "wide8p": "k_wide8_packet"}.get(
+            kern, ("k_gi_" if wl.layout == A.LAYOUT_GI else "k_rs_") + kern)
+        rays_dom = sum(len(wl.batches[i].rays) for i in wl.groups[dom])
+        achieved = group_bytes[dom] / (group_ms[dom] * 1e-3) / 1e9
+        traffic = TRAFFIC.get((args.config, bool(args.small), name))
+        roof = dict(bound="hbm", achieved=achieved, peak=peak, unit="GB/s", frac=achieved / peak,
+                    traffic=traffic * rays_dom if traffic else None,
+                    kernel=name, launch="+".join(wl.batches[i].label for i in wl.groups[dom]),
+                    launch_ms=float(group_ms[dom]), share_of_step=float(group_ms[dom] / group_ms.sum()),
+                    peak_source=f"{peak_kind} hbm_gbs", bytes_per_ray=group_bytes[dom] / rays_dom,
+                    note="the longest launch of a step: its algorithmic bytes (visit counters) over its CUDA-event "
+                         "time; scenes under 126 MB are L2-resident, so the HBM fraction is a ceiling check, "
+                         "not the limit; traffic is ncu's DRAM bytes per ray on this launch, scaled to its rays")
+        if all(x is not None for x in group_bytes):
+            roof["step_achieved"] = sum(group_bytes) / (ms * 1e-3) / 1e9
     def launches(g, p):  # traversal kernels (and ray-key kernels) a step launches
         if p is None or p.desc["kernel"] == "plain":
             return sum(1 for i in g if len(wl.batches[i].rays))
