@@ -61,6 +61,7 @@ def parse(argv=None):
     ap.add_argument("--kernel", default="auto", help="auto: the autotuner's choice; or plain / fast / wide8")
     ap.add_argument("--refill", type=int, default=0, help="with --kernel fast/wide8: the wavefront width")
     ap.add_argument("--order", default="none", help="with --kernel fast/wide8: the sort key")
+    ap.add_argument("--stack", default="", help="with --kernel wide8: local or shared node-group stack")
     ap.add_argument("--cpu-seconds", type=float, default=10.0, help="target wall time of the CPU baseline sample")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--small", action="store_true", help="a reduced workload (profiling captures)")
@@ -623,7 +624,8 @@ def run_ours(args):
         elif args.kernel == "plain":
             plans.append(None)
         else:
-            plans.append(engine.plan(scene, batches, args.kernel, refill=args.refill, order=args.order))
+            plans.append(engine.plan(scene, batches, args.kernel, refill=args.refill, order=args.order,
+                                     stack=args.stack if args.kernel == "wide8" else ""))
     t_tune = time.perf_counter() - t_tune
 
     def plain_step():
@@ -710,8 +712,10 @@ def run_ours(args):
     def host_step():
         for g, p in zip(wl.groups, plans):
             kern = p.desc["kernel"] if p is not None else "plain"
-            if kern != "plain":
-                engine.set_tuning(**{f"{kern}_refill": p.desc["refill"] or 8})
+            if kern == "wide8":
+                engine.set_tuning(wide8_refill=p.desc["refill"] or 8, wide8_stack=A.STACKS[p.desc.get("stack", "local")])
+            elif kern == "fast":
+                engine.set_tuning(fast_refill=p.desc["refill"] or 8)
             for i in g:
                 engine.trace_host(scene, pinned[i], wl.batches[i].mode, kern, out=outs[i])
 

@@ -93,11 +93,18 @@ typedef struct rt_gi_hit {
 /* Any-hit results are one uint32 per ray: 1 when something blocks the ray, else 0
  * (gi_visible returns the negation). */
 
+/* Where the WIDE8 per-ray walk keeps each lane's node-group stack (rt_tuning.wide8_stack,
+ * rt_plan_desc.stack; 0 there means unchanged / the context's choice). No counterpart in the
+ * reference, whose WGSL loops keep a fixed array per invocation. */
+#define RT_STACK_LOCAL 1u  /* 32 entries a lane in local memory, cached by L1 (the default) */
+#define RT_STACK_SHARED 2u /* 16 entries a lane in shared memory: only for scenes whose 8-wide trees are
+                            * at most 16 levels deep (else RT_ERR_UNSUPPORTED) */
 /* Launch parameters the autotuner chooses (renderlab_b200.tune); zero fields keep defaults. */
 typedef struct rt_tuning {
   uint32_t fast_refill;  /* FAST: idle lanes (1-32) a persistent warp waits for before taking more rays */
   uint32_t wide8_refill; /* WIDE8: the same */
-  uint32_t reserved[6];
+  uint32_t wide8_stack;  /* WIDE8: RT_STACK_LOCAL or RT_STACK_SHARED */
+  uint32_t reserved[5];
 } rt_tuning;
 
 typedef struct rt_ctx rt_ctx;
@@ -141,6 +148,9 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
 /* Builds the derived layout a kernel needs (RT_KERNEL_WIDE8: the compressed 8-wide BVH over the
  * scene's triangles, built on the host threads and uploaded). PLAIN and FAST need nothing. */
 rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel);
+/* Levels of the deepest 8-wide BLAS (after rt_scene_prepare for WIDE8, else RT_ERR_UNSUPPORTED):
+ * RT_STACK_SHARED needs at most 16. */
+rt_status rt_scene_wide8_depth(const rt_scene* scene, uint32_t* depth);
 rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene);
 size_t rt_scene_device_bytes(const rt_scene* scene);
 
@@ -236,6 +246,7 @@ typedef struct rt_plan_desc {
   uint32_t refill;    /* idle lanes (1-32) before a warp takes more rays; 0: the context's tuning */
   rt_ray_order order; /* sort the launch's rays first (RT_ORDER_NONE: no sort; PLAIN takes none) */
   uint32_t graph;     /* 1: replay a captured CUDA graph; 0: launch directly */
+  uint32_t stack;     /* WIDE8: RT_STACK_LOCAL or RT_STACK_SHARED; 0: the context's tuning */
 } rt_plan_desc;
 rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_batches, uint32_t n_batches,
                          const rt_plan_desc* desc, rt_plan** out);

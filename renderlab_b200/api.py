@@ -28,6 +28,7 @@ LAYOUT_GI, LAYOUT_REFLECTION, LAYOUT_REFLECTION_BVH2 = 0, 1, 2
 CLOSEST, ANY_SKY, ANY_CASTERS = 0, 1, 2
 KERNELS = {"plain": 0, "fast": 1, "wide8": 2, "wide8p": 3}
 ORDERS = {"none": 0, "origin": 1, "octant": 2, "direction": 3}
+STACKS = {"": 0, "local": 1, "shared": 2}  # RT_STACK_LOCAL / RT_STACK_SHARED
 STATUS = {0: "OK", 1: "INVALID_ARG", 2: "LAYOUT", 3: "OOM", 4: "STACK_OVERFLOW", 5: "TIMEOUT",
           6: "CUDA", 7: "BUSY", 8: "UNSUPPORTED"}
 GI_HIT_WORDS, RS_HIT_WORDS = 10, 5
@@ -61,7 +62,8 @@ class RtBatch(ctypes.Structure):
 
 
 class RtPlanDesc(ctypes.Structure):
-    _fields_ = [("kernel", ctypes.c_int), ("refill", ctypes.c_uint32), ("order", ctypes.c_int), ("graph", ctypes.c_uint32)]
+    _fields_ = [("kernel", ctypes.c_int), ("refill", ctypes.c_uint32), ("order", ctypes.c_int), ("graph", ctypes.c_uint32),
+                ("stack", ctypes.c_uint32)]
 
 
 class RtServerDesc(ctypes.Structure):
@@ -86,7 +88,8 @@ class RtRnfPlacement(ctypes.Structure):
 
 
 class RtTuning(ctypes.Structure):
-    _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 6)]
+    _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("wide8_stack", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32 * 5)]
 
 
 EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",
@@ -96,7 +99,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
-           "rt_trace_static", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
+           "rt_trace_static", "rt_scene_wide8_depth", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
            "rt_rnf_placement_get", "rt_rnf_encode", "rt_rnf_pack_gi", "rt_rnf_world", "rt_rnf_free")
@@ -128,6 +131,7 @@ def lib() -> ctypes.CDLL:
     L.rt_scene_update_records.argtypes = [_vp, _vp, _u32p, ctypes.c_size_t]
     L.rt_scene_release.argtypes = [_vp, _vp]
     L.rt_scene_prepare.argtypes = [_vp, _vp, ctypes.c_int]
+    L.rt_scene_wide8_depth.argtypes = [_vp, _u32p]
     L.rt_scene_device_bytes.argtypes = [_vp]
     L.rt_scene_device_bytes.restype = ctypes.c_size_t
     L.rt_trace.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
@@ -360,6 +364,12 @@ class Scene:
         """Build the derived layout `kernel` reads (the 8-wide BVH for "wide8")."""
         self.engine._check(lib().rt_scene_prepare(self.engine.ctx, self.handle, KERNELS[kernel]))
 
+    def wide8_depth(self) -> int:
+        """Levels of the deepest 8-wide BLAS (after prepare("wide8")); the shared stack takes 16."""
+        d = ctypes.c_uint32()
+        self.engine._check(lib().rt_scene_wide8_depth(self.handle, ctypes.byref(d)))
+        return int(d.value)
+
     def refit(self, instance: int, positions, indices=None, stream=None):
         """rt_scene_refit: new positions (CUDA float32 tensor (V, 3)) for the BLAS of `instance`;
         the reflection layout also takes the mesh's triangle list (CUDA int32/uint32 tensor)."""
@@ -581,14 +591,17 @@ class Engine:
         return outs
 
     def plan(self, scene: Scene, batches, kernel: str = "fast", refill: int = 0, order: str = "none",
-             graph: bool = True) -> "Plan":
-        """A prepared many-batch launch over fixed buffers (see rt_plan_create)."""
+             graph: bool = True, stack: str = "") -> "Plan":
+        """A prepared many-batch launch over fixed buffers (see rt_plan_create). `stack`: where
+        WIDE8 keeps each lane's node-group stack, "local" or "shared" ("": the context's tuning)."""
         arr, outs = self._batch_array(scene, batches)
-        desc = RtPlanDesc(KERNELS[kernel], refill, ORDERS[order], 1 if graph else 0)
+        desc = RtPlanDesc(KERNELS[kernel], refill, ORDERS[order], 1 if graph else 0, STACKS[stack])
         h = _vp()
         self._check(lib().rt_plan_create(self.ctx, scene.handle, arr, len(batches), ctypes.byref(desc), ctypes.byref(h)))
-        return Plan(self, scene, h, outs, [b[0] for b in batches], dict(kernel=kernel, refill=refill, order=order,
-                                                                          graph=graph))
+        desc = dict(kernel=kernel, refill=refill, order=order, graph=graph)
+        if stack:
+            desc["stack"] = stack
+        return Plan(self, scene, h, outs, [b[0] for b in batches], desc)
 
     def gi_cell_rays(self, cells, rotate: bool = False, stream=None):
         """The GI cache cells' 64 fixed-direction rays each: cells (n, 8) int32 CUDA tensor of

@@ -72,10 +72,11 @@ cudaError_t enqueue_plain(const rt_scene* scene, const rtk::BatchEntry* h_table,
 
 cudaError_t enqueue(const rt_scene* scene, rt_kernel kernel, const rtk::BatchEntry* d_table, uint32_t entries,
                     uint32_t total, const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t s,
-                    uint32_t refill, int uniform) {
+                    uint32_t refill, int uniform, uint32_t stack) {
   const rtl::SceneView v = view_of(scene);
   if (kernel == RT_KERNEL_WIDE8)
-    return rtl::launch_wide8_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform);
+    return rtl::launch_wide8_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform,
+                                     stack == RT_STACK_SHARED ? 1u : 0u);
   if (kernel == RT_KERNEL_WIDE8_PACKET)
     return rtl::launch_wide8_packet_batches(v, d_table, entries, total, order, counter, st, s, uniform);
   return rtl::launch_fast_batches(v, d_table, entries, total, order, counter, st, s, refill, uniform);
@@ -125,8 +126,12 @@ rt_status rt_trace_batches(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel,
   RT_CUDA(ctx, cudaMemcpyAsync(d, h, sizeof(rtk::BatchEntry) * n_batches, cudaMemcpyHostToDevice, s));
   RT_CUDA(ctx, cudaEventRecord(ctx->table_done[slot], s));
   const uint32_t refill = kernel == RT_KERNEL_FAST ? ctx->tuning.fast_refill : ctx->tuning.wide8_refill;
+  if (kernel == RT_KERNEL_WIDE8 && ctx->tuning.wide8_stack == RT_STACK_SHARED && !rtl::shared_stack_fits(view_of(scene)))
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the shared group stack holds 16 levels; this scene's 8-wide trees have %u",
+                scene->w8_depth);
   cudaError_t e = enqueue(scene, kernel, d, n_batches, (uint32_t)total, nullptr,
-                          ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, s, refill, uniform);
+                          ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, s, refill, uniform,
+                          ctx->tuning.wide8_stack);
   if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "many-batch launch: %s", cudaGetErrorString(e));
   ctx->rays += total;
   ctx->launches += 1;
@@ -137,7 +142,7 @@ struct rt_plan {
   rt_ctx* ctx = nullptr;
   const rt_scene* scene = nullptr;
   rt_plan_desc desc{};
-  uint32_t entries = 0, total = 0, refill = 8;
+  uint32_t entries = 0, total = 0, refill = 8, stack = RT_STACK_LOCAL;
   int uniform = -1;
   rtk::BatchEntry* d_table = nullptr;
   unsigned int* d_counter = nullptr;
@@ -162,7 +167,7 @@ cudaError_t plan_enqueue(const rt_plan* p, cudaStream_t s) {
     if (e != cudaSuccess) return e;
   }
   return enqueue(p->scene, p->desc.kernel, p->d_table, p->entries, p->total, p->d_order, p->d_counter,
-                 p->ctx->d_status, s, p->refill, p->uniform);
+                 p->ctx->d_status, s, p->refill, p->uniform, p->stack);
 }
 
 void plan_free(rt_plan* p) {
@@ -185,6 +190,7 @@ rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_b
   if (desc->refill > 32) return fail(ctx, RT_ERR_INVALID_ARG, "refill thresholds are 1-32 lanes");
   if (desc->kernel == RT_KERNEL_PLAIN && desc->order != RT_ORDER_NONE)
     return fail(ctx, RT_ERR_UNSUPPORTED, "the PLAIN kernel takes no ray order");
+  if (desc->stack > RT_STACK_SHARED) return fail(ctx, RT_ERR_INVALID_ARG, "unknown stack placement %u", desc->stack);
   std::vector<rtk::BatchEntry> table(n_batches ? n_batches : 1);
   uint64_t total = 0;
   int uniform = -1;
@@ -201,6 +207,13 @@ rt_status rt_plan_create(rt_ctx* ctx, const rt_scene* scene, const rt_batch* h_b
   p->h_table = table;
   p->refill = desc->refill ? desc->refill
                            : (desc->kernel == RT_KERNEL_FAST ? ctx->tuning.fast_refill : ctx->tuning.wide8_refill);
+  p->stack = desc->stack ? desc->stack : ctx->tuning.wide8_stack;
+  if (desc->kernel == RT_KERNEL_WIDE8 && p->stack == RT_STACK_SHARED && !rtl::shared_stack_fits(view_of(scene))) {
+    const uint32_t depth = scene->w8_depth;
+    delete p;
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the shared group stack holds 16 levels; this scene's 8-wide trees have %u",
+                depth);
+  }
   world_box(scene, p->lo, p->hi);
   auto oom = [&](const char* what, size_t bytes) {
     cudaGetLastError();

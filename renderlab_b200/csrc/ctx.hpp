@@ -34,6 +34,7 @@ struct rt_scene {
   void* d_wide8 = nullptr;
   size_t wide8_bytes = 0;
   size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
+  uint32_t w8_depth = 0;  // levels of the deepest 8-wide BLAS
   std::map<uint32_t, RefitLevels> refit;  // by the BLAS's node base word
 };
 
@@ -53,7 +54,7 @@ struct rt_ctx {
   // many launches may be in flight at once across streams.
   unsigned int* d_counters = nullptr;
   std::atomic<uint64_t> counter_seq{0};
-  rt_tuning tuning = {8, 8, {0, 0, 0, 0, 0, 0}};
+  rt_tuning tuning = {8, 8, RT_STACK_LOCAL, {0, 0, 0, 0, 0}};
   std::mutex mu;
   std::string last_error;
   std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
@@ -113,6 +114,7 @@ inline rtl::SceneView view_of(const rt_scene* s) {
   v.wide8 = s->d_wide8;
   v.wide8_bytes = s->wide8_bytes;
   v.w8_nodes_at = s->w8_nodes_at, v.w8_tris_at = s->w8_tris_at, v.w8_inst_at = s->w8_inst_at;
+  v.w8_depth = s->w8_depth;
   return v;
 }
 

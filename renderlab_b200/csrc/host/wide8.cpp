@@ -230,13 +230,14 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
   std::vector<BNode> bn = bin.nodes();
   const auto& refs = bin.refs();
   const Collapse plan(bn);
-  struct Task { uint32_t wide; int b; };
+  struct Task { uint32_t wide; int b; uint32_t level; };
   std::deque<Task> queue;
   out.nodes.resize(W8_NODE_WORDS, 0);
-  queue.push_back({0, broot});
+  queue.push_back({0, broot, 1});
   while (!queue.empty()) {
     const Task task = queue.front();
     queue.pop_front();
+    out.depth = std::max(out.depth, task.level);
     std::vector<int> kids;
     if (bn[task.b].count > 0) kids.push_back(task.b);  // a BLAS of one leaf
     else kids = plan.children(task.b);
@@ -324,7 +325,7 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
     }
     uint32_t next = child_base;
     for (int s = 0; s < 8; ++s)
-      if (slot_of[s] >= 0 && bn[kids[slot_of[s]]].count == 0) queue.push_back({next++, kids[slot_of[s]]});
+      if (slot_of[s] >= 0 && bn[kids[slot_of[s]]].count == 0) queue.push_back({next++, kids[slot_of[s]], task.level + 1});
   }
 }
 
@@ -429,6 +430,7 @@ bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8
   std::vector<uint32_t> node_base(nb), tri_base(nb);
   size_t nn = 0, ntri = 0;
   for (size_t b = 0; b < nb; ++b) {
+    out.depth = std::max(out.depth, built[b].depth);
     if (built[b].max_exponent > W8_MAX_EXPONENT) {
       err = "a BLAS extends beyond 255 * 2^13 units on an axis: its 8-wide nodes cannot be decoded exactly";
       return false;

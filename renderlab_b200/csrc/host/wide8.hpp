@@ -41,6 +41,7 @@ struct Wide8Blas {
   std::vector<uint32_t> nodes;  // root is node 0
   std::vector<uint32_t> tris;
   int max_exponent = -126;      // the largest scale exponent of its nodes
+  uint32_t depth = 0;           // levels of 8-wide nodes (a walk stacks at most depth - 1 groups)
 };
 
 // The whole derived scene: per distinct BLAS of the packed words, its nodes and triangles, and
@@ -50,6 +51,7 @@ struct Wide8Scene {
   std::vector<uint32_t> tris;
   std::vector<uint32_t> inst;  // 2 words per instance: node base, triangle base
   size_t blas_count = 0;
+  uint32_t depth = 0;  // the deepest BLAS's levels
 };
 
 // Source triangle for the builder: f32 vertices plus identity words.

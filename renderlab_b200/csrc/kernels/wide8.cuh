@@ -24,6 +24,9 @@ constexpr float W8_U = 5.9604645e-8f;  // 2^-24
 constexpr float W8_TIE = 8e-6f;
 constexpr float W8_EDGE = 1e-5f;
 constexpr uint32_t W8_STACK = 32;
+// Entries of the shared-memory group stack (a scene whose 8-wide trees are at most this many
+// levels deep stacks at most W8_SSTACK - 1 groups).
+constexpr uint32_t W8_SSTACK = 16;
 // Resident 128-thread blocks per SM the register allocation is sized for (4: 128 registers).
 #ifndef RT_W8_MIN_BLOCKS
 #define RT_W8_MIN_BLOCKS 4
@@ -340,8 +343,24 @@ RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, co
 
 // One 8-wide node: its leaf triangles are tested now, its inner hits become the group.
 // Returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, int AM, bool COUNT>
-RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint2* stack, DevStatus* st,
+// A lane's node-group stack: W8_STACK entries in local memory (cached by L1), or SS entries in a
+// shared-memory column of the block (entry i of thread t at i * BLOCK + t: the lanes of a warp
+// touch 32 consecutive words, so no bank conflict).
+template <int SS, int BLOCK>
+struct W8GroupStack {
+  uint2* col;
+  static constexpr uint32_t cap = SS;
+  RT_DEV uint2& operator[](uint32_t i) const { return col[i * BLOCK]; }
+};
+template <int BLOCK>
+struct W8GroupStack<0, BLOCK> {
+  uint2 e[W8_STACK];
+  static constexpr uint32_t cap = W8_STACK;
+  RT_DEV uint2& operator[](uint32_t i) { return e[i]; }
+};
+
+template <uint32_t LAYOUT, int AM, bool COUNT, class Stack>
+RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, Stack& stack, DevStatus* st,
                     unsigned long long* cnt) {
   w8_count<COUNT>(cnt, W8C_NODES);
   const W8Ray& R = L.R;
@@ -367,7 +386,7 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const uint32_t inner = oct_permute(hits & imask, R.oct);
   if (inner) {
     if (L.g_bits) {
-      if (L.sp < W8_STACK) stack[L.sp++] = make_uint2(L.g_base, L.g_bits | L.g_imask << 8);
+      if (L.sp < Stack::cap) stack[L.sp++] = make_uint2(L.g_base, L.g_bits | L.g_imask << 8);
       else atomicAdd(&st->stack_drops, 1ull);
     }
     L.g_base = child_base, L.g_bits = inner, L.g_imask = imask;
@@ -377,7 +396,8 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
 }
 
 // The next node of the current group (or of a popped one); false when the BLAS is done.
-RT_DEV bool w8_next(W8Lane& L, const uint2* stack) {
+template <class Stack>
+RT_DEV bool w8_next(W8Lane& L, Stack& stack) {
   while (L.g_bits == 0) {
     if (L.sp == 0) return false;
     const uint2 e = stack[--L.sp];
@@ -479,11 +499,15 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
 // Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
 // step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
 // re-converges at the top of the loop.
-template <uint32_t LAYOUT, int AM, int BLOCK, bool COUNT, class Src>
+template <uint32_t LAYOUT, int AM, int BLOCK, bool COUNT, class Src, int SS = 0>
 __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                  unsigned int* __restrict__ counter, uint32_t n, DevStatus* st,
                                                  unsigned long long* cnt, uint32_t refill) {
-  uint2 stack[W8_STACK];
+  W8GroupStack<SS, BLOCK> stack;
+  if constexpr (SS > 0) {
+    __shared__ uint2 columns[SS * BLOCK];
+    stack.col = columns + threadIdx.x;
+  }
   uint32_t tstack[STACK];
   W8Lane L;
   L.phase = 0;

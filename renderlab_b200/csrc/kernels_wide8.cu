@@ -1,4 +1,7 @@
 // Launchers for the WIDE8 kernels.
+#include <map>
+#include <mutex>
+
 #include "kernels/wide8.cuh"
 #include "launch.hpp"
 
@@ -8,18 +11,31 @@ namespace {
 constexpr int W8_BLOCK = 128;
 }
 
+// Resident blocks of `kernel` on the current device: one cache per kernel, since instances of one
+// signature (the same function-pointer type) can differ in registers and shared memory.
 template <class K>
 cudaError_t resident(K kernel, uint32_t& out) {
-  static uint32_t cached = 0;
-  if (!cached) {
-    int dev = 0, sms = 0, per_sm = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, W8_BLOCK, 0);
-    if (e != cudaSuccess) return e;
-    cached = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, uint32_t> cached;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cached.find(key);
+    if (it != cached.end()) {
+      out = it->second;
+      return cudaSuccess;
+    }
   }
-  out = cached;
+  int sms = 0, per_sm = 0;
+  e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, W8_BLOCK, 0);
+  if (e != cudaSuccess) return e;
+  out = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+  std::lock_guard<std::mutex> lock(mu);
+  cached[key] = out;
   return cudaSuccess;
 }
 
@@ -44,7 +60,7 @@ bool view_of(const SceneView& s, rtk::W8View& v) {
   return true;
 }
 
-template <bool COUNT>
+template <bool COUNT, int SS>
 cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
                        unsigned long long* cnt, uint32_t refill) {
@@ -54,34 +70,46 @@ cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, co
   using rtk::OneBatch;
   const OneBatch src{rays, order, hits};
   if (s.layout == 0) {
-    if (mode == 0) return run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
-    return run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
+    if (mode == 0) return run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
+    return run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
   }
-  if (mode == 0) return run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
-  return run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch>, s.words, v, src, counter, n, st, stream, cnt, refill);
+  if (mode == 0) return run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
+  return run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
 }
 
+bool shared_stack_fits(const SceneView& s) { return s.w8_depth <= rtk::W8_SSTACK; }
+
 cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill) {
-  return launch_any<false>(s, mode, rays, order, hits, n, counter, st, stream, nullptr, refill);
+                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill,
+                         uint32_t stack) {
+  if (stack == 0) return launch_any<false, 0>(s, mode, rays, order, hits, n, counter, st, stream, nullptr, refill);
+  if (!shared_stack_fits(s)) return cudaErrorInvalidValue;
+  return launch_any<false, (int)rtk::W8_SSTACK>(s, mode, rays, order, hits, n, counter, st, stream, nullptr, refill);
 }
 
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream) {
-  return launch_any<true>(s, mode, rays, nullptr, hits, n, counter, st, stream, cnt, 1);
+  return launch_any<true, 0>(s, mode, rays, nullptr, hits, n, counter, st, stream, cnt, 1);
 }
 
 cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
                                  const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
-                                 uint32_t refill, int uniform_mode) {
+                                 uint32_t refill, int uniform_mode, uint32_t stack) {
   if (total == 0) return cudaSuccess;
   rtk::W8View v;
   if (!view_of(s, v)) return cudaErrorInvalidValue;
   using rtk::ManyBatches;
   const ManyBatches src{table, entries, order};
-#define RT_W8B(L, AM) run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches>, s.words, v, src, counter, total, st, stream, nullptr, refill)
-  if (s.layout == 0) return uniform_mode == 0 ? RT_W8B(0, 0) : (uniform_mode == 1 ? RT_W8B(0, 1) : RT_W8B(0, 2));
-  return uniform_mode == 0 ? RT_W8B(1, 0) : (uniform_mode == 1 ? RT_W8B(1, 1) : RT_W8B(1, 2));
+#define RT_W8B(L, AM, SS) \
+  run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches, SS>, s.words, v, src, counter, total, st, stream, nullptr, refill)
+  if (stack == 0) {
+    if (s.layout == 0) return uniform_mode == 0 ? RT_W8B(0, 0, 0) : (uniform_mode == 1 ? RT_W8B(0, 1, 0) : RT_W8B(0, 2, 0));
+    return uniform_mode == 0 ? RT_W8B(1, 0, 0) : (uniform_mode == 1 ? RT_W8B(1, 1, 0) : RT_W8B(1, 2, 0));
+  }
+  if (!shared_stack_fits(s)) return cudaErrorInvalidValue;
+  constexpr int SS = (int)rtk::W8_SSTACK;
+  if (s.layout == 0) return uniform_mode == 0 ? RT_W8B(0, 0, SS) : (uniform_mode == 1 ? RT_W8B(0, 1, SS) : RT_W8B(0, 2, SS));
+  return uniform_mode == 0 ? RT_W8B(1, 0, SS) : (uniform_mode == 1 ? RT_W8B(1, 1, SS) : RT_W8B(1, 2, SS));
 #undef RT_W8B
 }
 

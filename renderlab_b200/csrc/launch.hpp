@@ -19,6 +19,7 @@ struct SceneView {
   const void* wide8;
   size_t wide8_bytes;
   size_t w8_nodes_at, w8_tris_at, w8_inst_at;
+  uint32_t w8_depth;  // levels of the deepest 8-wide BLAS
 };
 
 // PLAIN: mode 0 closest, 1/2 any-hit. Hits as documented in rt_trace.h.
@@ -29,9 +30,13 @@ cudaError_t launch_plain(const SceneView& s, uint32_t mode, const float4* rays, 
 cudaError_t launch_fast(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
 // WIDE8: the precision variant over the scene's derived 8-wide layout.
-// `refill`: idle lanes (1-32) a warp waits for before it takes more rays.
+// `refill`: idle lanes (1-32) a warp waits for before it takes more rays. `stack`: 0 keeps each
+// lane's node-group stack in local memory (32 entries), 1 in shared memory (16 entries: only for
+// scenes whose 8-wide trees are at most 16 levels deep, else cudaErrorInvalidValue).
 cudaError_t launch_wide8(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
-                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
+                         uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill,
+                         uint32_t stack);
+bool shared_stack_fits(const SceneView& s);
 // Many batches in one persistent launch: `table` (device, `entries` records sorted by `first`)
 // covers `total` rays; `order` (optional) permutes the launch's ray space. Mode per entry;
 // `uniform_mode` 0 / 1 when every non-empty entry is closest / any hit (a kernel with the mode
@@ -41,7 +46,7 @@ cudaError_t launch_fast_batches(const SceneView& s, const rtk::BatchEntry* table
                                 uint32_t refill, int uniform_mode);
 cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries, uint32_t total,
                                  const uint32_t* order, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
-                                 uint32_t refill, int uniform_mode);
+                                 uint32_t refill, int uniform_mode, uint32_t stack);
 // WIDE8 with per-event device counters (rtk::W8Count order) accumulated into cnt[8].
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream);

@@ -40,9 +40,12 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
     case RT_KERNEL_WIDE8:
       if (!scene->d_wide8)
         return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
+      if (ctx->tuning.wide8_stack == RT_STACK_SHARED && !rtl::shared_stack_fits(v))
+        return fail(ctx, RT_ERR_UNSUPPORTED, "the shared group stack holds 16 levels; this scene's 8-wide trees have %u",
+                    v.w8_depth);
       e = rtl::launch_wide8(v, (uint32_t)mode, r, order, hits, n,
                             ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream,
-                            ctx->tuning.wide8_refill);
+                            ctx->tuning.wide8_refill, ctx->tuning.wide8_stack == RT_STACK_SHARED ? 1u : 0u);
       break;
     case RT_KERNEL_WIDE8_PACKET:
       if (!scene->d_wide8)
@@ -130,8 +133,10 @@ rt_status rt_ctx_set_tuning(rt_ctx* ctx, const rt_tuning* t) {
   rt_tuning next = ctx->tuning;
   for (uint32_t v : {t->fast_refill, t->wide8_refill})
     if (v > 32) return fail(ctx, RT_ERR_INVALID_ARG, "refill thresholds are 1-32 lanes");
+  if (t->wide8_stack > RT_STACK_SHARED) return fail(ctx, RT_ERR_INVALID_ARG, "unknown stack placement %u", t->wide8_stack);
   if (t->fast_refill) next.fast_refill = t->fast_refill;
   if (t->wide8_refill) next.wide8_refill = t->wide8_refill;
+  if (t->wide8_stack) next.wide8_stack = t->wide8_stack;
   ctx->tuning = next;
   return RT_OK;
 }
@@ -245,8 +250,16 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   scene->d_wide8 = d;
   scene->wide8_bytes = total * 4;
   scene->w8_nodes_at = nodes_at, scene->w8_tris_at = tris_at, scene->w8_inst_at = inst_at;
+  scene->w8_depth = w8.depth;
   scene->device_bytes += scene->wide8_bytes;
   ctx->scene_bytes += scene->wide8_bytes;
+  return RT_OK;
+}
+
+rt_status rt_scene_wide8_depth(const rt_scene* scene, uint32_t* depth) {
+  if (!scene || !depth) return RT_ERR_INVALID_ARG;
+  if (!scene->d_wide8) return RT_ERR_UNSUPPORTED;
+  *depth = scene->w8_depth;
   return RT_OK;
 }
 

@@ -88,7 +88,11 @@ def test_validation_rejects_unsafe_words():
 def test_tuner_candidates_cover_the_grid_once():
     from renderlab_b200 import tune as T
     c = T.candidates()
-    assert len(c) == len(set(c)) == (len(T.KERNELS) - 2) * len(T.REFILLS) * len(T.ORDERS) + 1 + len(T.ORDERS)
-    assert [x for x in c if x[0] == "plain"] == [("plain", 0, "none")]
+    assert len(c) == len(set(c)) == ((len(T.KERNELS) - 2) * len(T.REFILLS) * len(T.ORDERS) + 1 + len(T.ORDERS)
+                                     + len(T.REFILLS) * (len(T.STACKS) - 1))
+    assert [x for x in c if x[0] == "plain"] == [("plain", 0, "none", "")]
     assert {x[1] for x in c if x[0] == "wide8p"} == {32}
     assert c[0][2] == "none" and c[-1][2] != "none"
+    # the stack choice is WIDE8's alone, and its shared stack is tried unsorted
+    assert {x[3] for x in c if x[0] == "wide8"} == set(T.STACKS) and {x[3] for x in c if x[0] != "wide8"} == {""}
+    assert {x[2] for x in c if x[3] == "shared"} == {"none"}

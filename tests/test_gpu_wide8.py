@@ -239,3 +239,41 @@ def test_wide8_far_small_triangles_near_edges(engine, w8kernel):
         ref, ident = O.fp64_trace(w, rays, layout)
         check_closest(layout, got, ref, ident, f"near edges, layout {layout}")
         assert 0.3 < (ref[:, 0] > 0).mean() < 0.7
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_shared_group_stack_gives_the_local_stack_results(engine, layout):
+    """WIDE8's per-ray walk with each lane's node-group stack in shared memory (16 entries)
+    writes word for word what the local-memory stack writes -- through plans and through the
+    context's tuning, closest and any hit, primaries and incoherent rays -- and drops no push."""
+    import torch
+    mesh, rays = H.small_clusters(60_000, 256, 256)
+    prims = [True] if layout == A.LAYOUT_GI else None
+    w = product_words(layout, [mesh], S.identity_instances(1), primitives=prims)
+    scene = engine.upload(layout, w)
+    drops = engine.stats()["stack_overflows"]
+    try:
+        scene.prepare("wide8")
+        assert 1 <= scene.wide8_depth() <= 16
+        rnd = H.random_rays(30_000, -120.0, 120.0, seed=6, tmax=400.0)
+        d, e = torch.from_numpy(rays).cuda(), torch.from_numpy(rnd).cuda()
+        batches = [(d, A.CLOSEST), (e, A.CLOSEST), (e[:7000], A.ANY_CASTERS)]
+        plans = {s: engine.plan(scene, batches, "wide8", refill=8, stack=s) for s in ("local", "shared")}
+        for p in plans.values():
+            p.launch()
+        torch.cuda.synchronize()
+        for a, b in zip(plans["local"].hits, plans["shared"].hits):
+            assert torch.equal(a, b)
+        want = [engine.trace(scene, r, m, "wide8") for r, m in batches]
+        engine.set_tuning(wide8_stack=A.STACKS["shared"])
+        got = [engine.trace(scene, r, m, "wide8") for r, m in batches]
+        engine.set_tuning(wide8_stack=A.STACKS["local"])
+        torch.cuda.synchronize()
+        for a, b, p in zip(want, got, plans["local"].hits):
+            assert torch.equal(a, b) and torch.equal(a, p)
+        for p in plans.values():
+            p.close()
+        assert engine.stats()["stack_overflows"] == drops
+    finally:
+        engine.set_tuning(wide8_stack=A.STACKS["local"])
+        scene.release()
