@@ -300,6 +300,20 @@ rt_status rt_server_destroy(rt_server* srv);
  * over two streams. Returns when the hits are in h_hits. */
 rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
                         const rt_ray* h_rays, void* h_hits, uint32_t n);
+/* Several host-buffer batches, each with its own mode and kernel, in one pipeline: the chunks of
+ * all batches go through the same two streams in order, so one batch's first copy overlaps the
+ * previous batch's last kernel (a frame's shadow, GI and reflection rays in one call). Returns
+ * when every batch's hits are in its h_hits. No counterpart in the reference (its passes
+ * dispatch on the GPU queue). */
+typedef struct rt_host_batch {
+  const rt_ray* h_rays;
+  void* h_hits;
+  uint32_t n;
+  rt_mode mode;
+  rt_kernel kernel;
+} rt_host_batch;
+rt_status rt_trace_host_batches(rt_ctx* ctx, const rt_scene* scene, const rt_host_batch* batches,
+                                uint32_t n_batches);
 rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays);
 /* rt_trace_ex in an instrumented build that counts, over the batch, into counts[8]:
  * rays, top-level nodes, instance box tests, BLAS nodes, leaves, triangles tested, f64

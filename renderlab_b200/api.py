@@ -61,6 +61,11 @@ class RtBatch(ctypes.Structure):
     _fields_ = [("d_rays", ctypes.c_void_p), ("d_hits", ctypes.c_void_p), ("n", ctypes.c_uint32), ("mode", ctypes.c_int)]
 
 
+class RtHostBatch(ctypes.Structure):
+    _fields_ = [("h_rays", ctypes.c_void_p), ("h_hits", ctypes.c_void_p), ("n", ctypes.c_uint32),
+                ("mode", ctypes.c_int), ("kernel", ctypes.c_int)]
+
+
 class RtPlanDesc(ctypes.Structure):
     _fields_ = [("kernel", ctypes.c_int), ("refill", ctypes.c_uint32), ("order", ctypes.c_int), ("graph", ctypes.c_uint32),
                 ("stack", ctypes.c_uint32)]
@@ -95,7 +100,7 @@ class RtTuning(ctypes.Structure):
 EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",
            "rt_ctx_set_tuning", "rt_ctx_get_tuning",
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
-           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
+           "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_trace_host_batches", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
@@ -137,6 +142,7 @@ def lib() -> ctypes.CDLL:
     L.rt_trace.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_ex.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_host.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32]
+    L.rt_trace_host_batches.argtypes = [_vp, _vp, ctypes.POINTER(RtHostBatch), ctypes.c_uint32]
     L.rt_ctx_reserve.argtypes = [_vp, ctypes.c_uint32]
     L.rt_order_rays.argtypes = [_vp, _vp, _vp, ctypes.c_uint32, ctypes.c_int, _vp, _vp]
     L.rt_trace_batches.argtypes = [_vp, _vp, ctypes.c_int, ctypes.POINTER(RtBatch), ctypes.c_uint32, _vp]
@@ -563,6 +569,25 @@ class Engine:
         hp = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
         self._check(lib().rt_trace_host(self.ctx, scene.handle, mode, KERNELS[kernel], rp, hp, n))
         return out
+
+    def trace_host_batches(self, scene: Scene, batches):
+        """Host-buffer batches in one pipeline: (rays, mode, kernel[, out]) tuples, rays numpy or
+        pinned torch CPU tensors; returns the hit arrays (the given `out`s where passed)."""
+        arr = (RtHostBatch * max(1, len(batches)))()
+        outs = []
+        for k, b in enumerate(batches):
+            rays, mode, kernel = b[0], b[1], b[2]
+            out = b[3] if len(b) > 3 and b[3] is not None else None
+            n = len(rays)
+            if out is None:
+                words = hit_words(scene.layout, mode)
+                out = np.zeros((n, words) if words > 1 else (n,), np.uint32)
+            outs.append(out)
+            arr[k].h_rays = rays.data_ptr() if hasattr(rays, "data_ptr") else rays.ctypes.data
+            arr[k].h_hits = out.data_ptr() if hasattr(out, "data_ptr") else out.ctypes.data
+            arr[k].n, arr[k].mode, arr[k].kernel = n, mode, KERNELS[kernel]
+        self._check(lib().rt_trace_host_batches(self.ctx, scene.handle, arr, len(batches)))
+        return outs
 
     def _batch_array(self, scene: Scene, batches):
         """(rays, mode[, hits]) tuples -> (ctypes RtBatch array, hit tensors)."""

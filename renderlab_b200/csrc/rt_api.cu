@@ -377,31 +377,51 @@ rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays) {
   return RT_OK;
 }
 
-rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* h_rays,
-                        void* h_hits, uint32_t n) {
-  rt_status s = check_trace_args(ctx, scene, mode, kernel);
+rt_status rt_trace_host_batches(rt_ctx* ctx, const rt_scene* scene, const rt_host_batch* batches,
+                                uint32_t n_batches) {
+  if (!ctx || (n_batches && !batches)) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  uint32_t most = 0;
+  for (uint32_t k = 0; k < n_batches; ++k) {
+    const rt_host_batch& hb = batches[k];
+    rt_status s = check_trace_args(ctx, scene, hb.mode, hb.kernel);
+    if (s != RT_OK) return s;
+    if (hb.n && (!hb.h_rays || !hb.h_hits)) return fail(ctx, RT_ERR_INVALID_ARG, "null ray or hit buffer");
+    most = std::max(most, hb.n);
+  }
+  if (most == 0) return RT_OK;
+  rt_status s = rt_ctx_reserve(ctx, most);
   if (s != RT_OK) return s;
-  if (n == 0) return RT_OK;
-  if (!h_rays || !h_hits) return fail(ctx, RT_ERR_INVALID_ARG, "null ray or hit buffer");
-  if ((s = rt_ctx_reserve(ctx, n)) != RT_OK) return s;
   std::lock_guard<std::mutex> lock(ctx->mu);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));
-  const size_t hb = hit_bytes(scene->layout, (uint32_t)mode);
   const uint32_t chunk = (uint32_t)ctx->stage_rays;
-  for (uint32_t off = 0, c = 0; off < n; off += chunk, ++c) {
-    const uint32_t m = std::min(chunk, n - off);
-    const int b = c & 1;
-    cudaStream_t st = ctx->streams[b];
-    char* dr = static_cast<char*>(ctx->d_rays) + (size_t)b * chunk * RAY_BYTES;
-    char* dh = static_cast<char*>(ctx->d_hits) + (size_t)b * chunk * GI_HIT_BYTES;
-    RT_CUDA(ctx, cudaMemcpyAsync(dr, h_rays + off, (size_t)m * RAY_BYTES, cudaMemcpyHostToDevice, st));
-    rt_status d = dispatch(ctx, scene, mode, kernel, reinterpret_cast<const rt_ray*>(dr), nullptr, dh, m, st);
-    if (d != RT_OK) return d;
-    RT_CUDA(ctx, cudaMemcpyAsync(static_cast<char*>(h_hits) + (size_t)off * hb, dh, (size_t)m * hb,
-                                 cudaMemcpyDeviceToHost, st));
+  uint32_t c = 0;  // chunks alternate between the two streams and staging halves across batches
+  for (uint32_t k = 0; k < n_batches; ++k) {
+    const rt_host_batch& hb = batches[k];
+    const size_t bytes = hit_bytes(scene->layout, (uint32_t)hb.mode);
+    for (uint32_t off = 0; off < hb.n; off += chunk, ++c) {
+      const uint32_t m = std::min(chunk, hb.n - off);
+      const int b = c & 1;
+      cudaStream_t st = ctx->streams[b];
+      char* dr = static_cast<char*>(ctx->d_rays) + (size_t)b * chunk * RAY_BYTES;
+      char* dh = static_cast<char*>(ctx->d_hits) + (size_t)b * chunk * GI_HIT_BYTES;
+      RT_CUDA(ctx, cudaMemcpyAsync(dr, hb.h_rays + off, (size_t)m * RAY_BYTES, cudaMemcpyHostToDevice, st));
+      rt_status d = dispatch(ctx, scene, hb.mode, hb.kernel, reinterpret_cast<const rt_ray*>(dr), nullptr, dh, m, st);
+      if (d != RT_OK) {
+        for (auto t : ctx->streams) cudaStreamSynchronize(t);
+        return d;
+      }
+      RT_CUDA(ctx, cudaMemcpyAsync(static_cast<char*>(hb.h_hits) + (size_t)off * bytes, dh, (size_t)m * bytes,
+                                   cudaMemcpyDeviceToHost, st));
+    }
   }
   for (auto st : ctx->streams) RT_CUDA(ctx, cudaStreamSynchronize(st));
   return RT_OK;
+}
+
+rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel, const rt_ray* h_rays,
+                        void* h_hits, uint32_t n) {
+  const rt_host_batch one{h_rays, h_hits, n, mode, kernel};
+  return rt_trace_host_batches(ctx, scene, &one, 1);
 }
 
 // ---------------------------------------------------------------- host builders

@@ -221,6 +221,15 @@ def test_host_buffers_match_device(engine):
         assert np.array_equal(out.numpy().view(np.uint32), dev)
         host = engine.trace_host(scene, rays, A.ANY_CASTERS, "plain")
         assert np.array_equal(host, gpu_trace(engine, scene, rays, A.ANY_CASTERS, "plain"))
+        # several batches, kernels and modes in one pipeline, twice in a row, into the same buffers
+        half = rays[: len(rays) // 2]
+        want = [dev, gpu_trace(engine, scene, half, A.ANY_CASTERS, "fast"), gpu_trace(engine, scene, rays, A.CLOSEST, "fast")]
+        outs = [torch.empty((len(rays), 5), dtype=torch.int32).pin_memory(), None, None]
+        for _ in range(2):
+            got = engine.trace_host_batches(scene, [(pinned, A.CLOSEST, "plain", outs[0]), (half, A.ANY_CASTERS, "fast"),
+                                                    (rays, A.CLOSEST, "fast"), (rays[:0], A.CLOSEST, "plain")])
+            assert np.array_equal(got[0].numpy().view(np.uint32), want[0])
+            assert np.array_equal(got[1], want[1]) and np.array_equal(got[2], want[2]) and len(got[3]) == 0
     finally:
         scene.release()
 
