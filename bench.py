@@ -322,10 +322,29 @@ def cpu_baseline_leg(wl: Workload, target_s: float, threads=None):
     wall = time.perf_counter() - t0
     counts = [oracle_trace(wl.words, wl.layout, r, b.mode, counters=True, threads=threads)[1]
               for b, r in zip(wl.batches, sample)]
+    # the same traversal on one core, over a sample sized for about a tenth of the time
+    one, _ = sample_of(wl, int(max(1024, 0.1 * target_s / max(per_ray * threads, 1e-9))))
+    t0 = time.perf_counter()
+    for b, r in zip(wl.batches, one):
+        oracle_trace(wl.words, wl.layout, r, b.mode, threads=1)
+    one_wall = time.perf_counter() - t0
+    n_one = sum(len(r) for r in one)
+    # and the FP64 reference traversal (reference.rs restated) on at most 65,536 rays of the sample
+    from oracle import oracle as O
+    sub, _ = sample_of(wl, 65_536)
+    t0 = time.perf_counter()
+    for b, r in zip(wl.batches, sub):
+        if len(r):
+            O.fp64_trace(wl.words, r, wl.layout, any_hit=b.mode != 0, threads=threads)
+    f64_wall = time.perf_counter() - t0
+    n_f64 = sum(len(r) for r in sub)
     return dict(value=n / wall / 1e6, unit=UNIT, cores=threads, kind="port",
                 sample=f"{n:,} rays ({100 * frac:.2f} % of each batch of the step, strided), oracle "
                        f"{'gi_traverse' if wl.layout == 0 else 'rs_trace'} (scalar f32 C++) on {threads} threads, "
-                       f"{wall:.2f} s"), (counts, [len(r) for r in sample])
+                       f"{wall:.2f} s",
+                one_core=dict(value=n_one / one_wall / 1e6, unit=UNIT, rays=n_one),
+                fp64=dict(value=n_f64 / f64_wall / 1e6, unit=UNIT, rays=n_f64, cores=threads)), \
+        (counts, [len(r) for r in sample])
 
 
 def precision_report(wl: Workload, results: dict, n_sample: int) -> dict:
