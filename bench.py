@@ -314,12 +314,18 @@ def cpu_baseline_leg(wl: Workload, target_s: float, threads=None):
     for b, r in zip(wl.batches, probe):
         oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
     per_ray = (time.perf_counter() - t0) / sum(len(r) for r in probe)
-    sample, frac = sample_of(wl, int(max(4096, target_s / max(per_ray, 1e-9))))
+    def timed(n_rays):
+        smp, f = sample_of(wl, n_rays)
+        t0 = time.perf_counter()
+        for b, r in zip(wl.batches, smp):
+            oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
+        return smp, f, time.perf_counter() - t0
+
+    sample, frac, wall = timed(int(max(4096, target_s / max(per_ray, 1e-9))))
     n = sum(len(r) for r in sample)
-    t0 = time.perf_counter()
-    for b, r in zip(wl.batches, sample):
-        oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
-    wall = time.perf_counter() - t0
+    if wall < 0.5 * target_s and frac < 1.0:  # the small probe overstated the cost a ray: resize once
+        sample, frac, wall = timed(int(n * target_s / max(wall, 1e-3)))
+        n = sum(len(r) for r in sample)
     counts = [oracle_trace(wl.words, wl.layout, r, b.mode, counters=True, threads=threads)[1]
               for b, r in zip(wl.batches, sample)]
     # the same traversal on one core, over a sample sized for about a tenth of the time
