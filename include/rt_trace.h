@@ -151,6 +151,14 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel);
 /* Levels of the deepest 8-wide BLAS (after rt_scene_prepare for WIDE8, else RT_ERR_UNSUPPORTED):
  * RT_STACK_SHARED needs at most 16. */
 rt_status rt_scene_wide8_depth(const rt_scene* scene, uint32_t* depth);
+/* Builds the 8-wide layout of these words on the host, as rt_scene_prepare does, and checks what
+ * the WIDE8 kernels rely on: indices in range, each triangle in exactly one leaf, every child box
+ * enclosing the triangles below it in exact arithmetic, empty
+ * slots inverted, node exponents in the decodable range. No device needed. info: 8-wide nodes,
+ * triangles, deepest level, distinct BLAS. No counterpart in the reference (its runtime BVH is
+ * the 4-wide one). */
+rt_status rt_wide8_check(rt_layout layout, const uint32_t* words, size_t n_words, uint32_t info[4], char* err,
+                         size_t err_len);
 rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene);
 size_t rt_scene_device_bytes(const rt_scene* scene);
 

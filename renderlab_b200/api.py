@@ -104,7 +104,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
-           "rt_trace_static", "rt_scene_wide8_depth", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
+           "rt_trace_static", "rt_scene_wide8_depth", "rt_wide8_check", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
            "rt_rnf_placement_get", "rt_rnf_encode", "rt_rnf_pack_gi", "rt_rnf_world", "rt_rnf_free")
@@ -137,6 +137,7 @@ def lib() -> ctypes.CDLL:
     L.rt_scene_release.argtypes = [_vp, _vp]
     L.rt_scene_prepare.argtypes = [_vp, _vp, ctypes.c_int]
     L.rt_scene_wide8_depth.argtypes = [_vp, _u32p]
+    L.rt_wide8_check.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, _u32p, ctypes.c_char_p, ctypes.c_size_t]
     L.rt_scene_device_bytes.argtypes = [_vp]
     L.rt_scene_device_bytes.restype = ctypes.c_size_t
     L.rt_trace.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
@@ -313,6 +314,18 @@ def pack_scene(layout: int, meshes, instances, tlas_mode: int = -1, primitives=N
     if st != 0:
         raise RtError(st, "packing failed")
     return out
+
+
+def wide8_check(layout: int, words) -> dict:
+    """Builds the 8-wide layout on the host and checks it (rt_wide8_check); raises RtError(LAYOUT)
+    with the reason, else returns its node, triangle, depth and BLAS counts."""
+    w = np.ascontiguousarray(words, np.uint32)
+    info = np.zeros(4, np.uint32)
+    err = ctypes.create_string_buffer(256)
+    st = lib().rt_wide8_check(layout, _np_ptr(w, _u32p), len(w), _np_ptr(info, _u32p), err, len(err))
+    if st != 0:
+        raise RtError(st, err.value.decode())
+    return dict(zip(("nodes", "triangles", "depth", "blas"), map(int, info)))
 
 
 def validate(layout: int, words) -> dict:

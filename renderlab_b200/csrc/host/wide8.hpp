@@ -6,7 +6,8 @@
 //   3     exponent bytes ex | ey << 8 | ez << 16 (scale 2^(e-127), e - 127 <= 13), inner-child mask << 24
 //   4     index of the first inner child node (inner children are contiguous, in slot order)
 //   5     index of the first triangle (leaf children's triangles are contiguous, in slot order)
-//   6-7   meta byte per slot: leaf (count << 5 | offset), 0 for an inner or empty slot
+//   6-7   meta byte per slot: leaf (count << 5 | offset), 0 for an inner or empty slot; an empty
+//         slot's box is inverted (lower planes 255, upper 0), so no ray meets it
 //   8-19  child boxes: lo x, lo y, lo z, hi x, hi y, hi z, one byte per slot (two words each)
 // A child box is the real interval [p + q_lo * 2^e, p + q_hi * 2^e] per axis; the builder
 // rounds q outward in exact arithmetic, so it encloses the child's triangles exactly.
@@ -63,5 +64,9 @@ struct SrcTri {
 void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out);
 bool build_wide8_scene(uint32_t layout, const uint32_t* words, size_t n_words, Wide8Scene& out, std::string& err,
                        int threads);
+// Checks a built layout (wide8_check.cpp): ranges, one leaf per triangle, every child box
+// enclosing its child in exact arithmetic, inverted empty slots, the recorded depth. info: nodes,
+// triangles, depth, distinct BLAS.
+bool check_wide8_scene(const Wide8Scene& s, uint32_t info[4], std::string& err);
 
 }  // namespace rtb

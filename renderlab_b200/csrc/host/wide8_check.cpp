@@ -1,0 +1,117 @@
+// A host-side check of the engine's derived 8-wide layout (wide8.hpp): the properties the WIDE8
+// kernels rely on, verified node by node in exact arithmetic, so that the builder's output can be
+// tested without a GPU. The box rule is the one traversal needs: a ray that meets a triangle meets
+// every child box on the path to its leaf.
+#include <algorithm>
+#include <cmath>
+#include <set>
+
+#include "host.hpp"
+#include "wide8.hpp"
+
+namespace rtb {
+
+namespace {
+
+struct Extent {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  void grow(const double* l, const double* h) {
+    for (int a = 0; a < 3; ++a) lo[a] = std::min(lo[a], l[a]), hi[a] = std::max(hi[a], h[a]);
+  }
+  bool within(const double* l, const double* h) const {
+    for (int a = 0; a < 3; ++a)
+      if (lo[a] < l[a] || hi[a] > h[a]) return false;
+    return true;
+  }
+};
+
+uint32_t byte_of(const uint32_t* w, int plane, int s) { return (w[8 + 2 * plane + (s >> 2)] >> (8 * (s & 3))) & 255u; }
+
+// Checks the subtree at `node`; returns the box of its triangles' vertices through `ext`. A child
+// box must enclose its child's triangles (what a ray must not miss), not the child's own, larger,
+// outward-rounded child boxes.
+bool check_node(const Wide8Scene& s, uint32_t node, uint32_t level, std::vector<uint8_t>& seen_node,
+                std::vector<uint8_t>& seen_tri, uint32_t& depth, Extent& ext, std::string& err) {
+  const size_t nn = s.nodes.size() / W8_NODE_WORDS, nt = s.tris.size() / W8_TRI_WORDS;
+  if (node >= nn) return err = "node index out of range", false;
+  if (seen_node[node]) return err = "a node is reached twice", false;
+  seen_node[node] = 1;
+  depth = std::max(depth, level);
+  const uint32_t* w = &s.nodes[(size_t)node * W8_NODE_WORDS];
+  double p[3], scale[3];
+  for (int a = 0; a < 3; ++a) {
+    const int e = (int)((w[3] >> (8 * a)) & 255u) - 127;
+    if (e > W8_MAX_EXPONENT || e < -126) return err = "node scale exponent out of range", false;
+    p[a] = as_float(w[a]);
+    scale[a] = std::ldexp(1.0, e);
+    if (!std::isfinite(p[a])) return err = "non-finite node origin", false;
+  }
+  const uint32_t imask = w[3] >> 24, child_base = w[4], tri_base = w[5];
+  uint32_t next_offset = 0;
+  for (int slot = 0; slot < 8; ++slot) {
+    const uint32_t meta = ((slot < 4 ? w[6] : w[7]) >> (8 * (slot & 3))) & 255u;
+    const bool inner = (imask >> slot) & 1u;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) {  // exact: a float plus an integer times a power of two
+      lo[a] = p[a] + byte_of(w, a, slot) * scale[a];
+      hi[a] = p[a] + byte_of(w, 3 + a, slot) * scale[a];
+    }
+    if (!inner && meta == 0) {  // empty: an inverted box no ray meets
+      for (int a = 0; a < 3; ++a)
+        if (byte_of(w, a, slot) != 255 || byte_of(w, 3 + a, slot) != 0) return err = "empty slot is not inverted", false;
+      continue;
+    }
+    if (inner && meta != 0) return err = "a slot is both inner and a leaf", false;
+    for (int a = 0; a < 3; ++a)
+      if (lo[a] > hi[a]) return err = "child box lower plane above its upper plane", false;
+    Extent child;
+    if (inner) {
+      const uint32_t c = child_base + (uint32_t)__builtin_popcount(imask & ((1u << slot) - 1u));
+      if (c <= node) return err = "inner child not after its parent", false;
+      if (!check_node(s, c, level + 1, seen_node, seen_tri, depth, child, err)) return false;
+    } else {
+      const uint32_t count = meta >> 5, offset = meta & 31u;
+      if (count > W8_MAX_LEAF) return err = "leaf holds more triangles than the builder allows", false;
+      if (offset != next_offset) return err = "leaf triangles not contiguous in slot order", false;
+      next_offset = offset + count;
+      for (uint32_t k = 0; k < count; ++k) {
+        const size_t t = (size_t)tri_base + offset + k;
+        if (t >= nt) return err = "triangle index out of range", false;
+        if (seen_tri[t]++) return err = "a triangle is referenced by two leaves", false;
+        const uint32_t* tw = &s.tris[t * W8_TRI_WORDS];
+        for (int v = 0; v < 3; ++v) {
+          double x[3];
+          for (int a = 0; a < 3; ++a) x[a] = as_float(tw[3 * v + a]);
+          child.grow(x, x);
+        }
+      }
+    }
+    if (!child.within(lo, hi)) return err = "a child box does not enclose its child's triangles", false;
+    ext.grow(child.lo, child.hi);
+  }
+  return true;
+}
+
+}  // namespace
+
+bool check_wide8_scene(const Wide8Scene& s, uint32_t info[4], std::string& err) {
+  const size_t nn = s.nodes.size() / W8_NODE_WORDS, nt = s.tris.size() / W8_TRI_WORDS;
+  std::vector<uint8_t> seen_node(nn, 0), seen_tri(nt, 0);
+  std::set<uint32_t> roots;
+  for (size_t i = 0; i + 1 < s.inst.size(); i += 2)
+    if (s.inst[i] != EMPTY) roots.insert(s.inst[i]);
+  uint32_t depth = 0;
+  for (uint32_t r : roots) {
+    Extent ext;
+    uint32_t d = 0;
+    if (!check_node(s, r, 1, seen_node, seen_tri, d, ext, err)) return false;
+    depth = std::max(depth, d);
+  }
+  if (std::find(seen_node.begin(), seen_node.end(), 0) != seen_node.end()) return err = "an unreachable node", false;
+  if (std::find(seen_tri.begin(), seen_tri.end(), 0) != seen_tri.end()) return err = "a triangle no leaf holds", false;
+  if (depth != s.depth) return err = "recorded depth differs from the tree's", false;
+  info[0] = (uint32_t)nn, info[1] = (uint32_t)nt, info[2] = depth, info[3] = (uint32_t)s.blas_count;
+  return true;
+}
+
+}  // namespace rtb

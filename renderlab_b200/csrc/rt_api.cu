@@ -256,6 +256,20 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   return RT_OK;
 }
 
+rt_status rt_wide8_check(rt_layout layout, const uint32_t* words, size_t n_words, uint32_t info[4], char* err,
+                         size_t err_len) {
+  if (!words || !info || (unsigned)layout > 1u) return RT_ERR_INVALID_ARG;
+  std::string why;
+  rtb::SceneInfo si;
+  rtb::Wide8Scene w8;
+  const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
+  bool ok = rtb::validate_scene((uint32_t)layout, words, n_words, si, why) &&
+            rtb::build_wide8_scene((uint32_t)layout, words, n_words, w8, why, threads) &&
+            rtb::check_wide8_scene(w8, info, why);
+  if (!ok && err && err_len) std::snprintf(err, err_len, "%s", why.c_str());
+  return ok ? RT_OK : RT_ERR_LAYOUT;
+}
+
 rt_status rt_scene_wide8_depth(const rt_scene* scene, uint32_t* depth) {
   if (!scene || !depth) return RT_ERR_INVALID_ARG;
   if (!scene->d_wide8) return RT_ERR_UNSUPPORTED;
