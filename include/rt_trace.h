@@ -386,6 +386,27 @@ rt_status rt_pack_scene(rt_layout layout, const rt_blas* const* meshes, uint32_t
                         const rt_instance* instances, uint32_t n_instances, int tlas_mode,
                         uint32_t* out_words, size_t* n_words);
 
+/* The object box rt_pack_scene places for a mesh (6 floats: lo xyz, hi xyz): GI, every position
+ * of the BLAS (gi_bvh.rs:70); reflection, the vertices of the source triangle list
+ * (reflection_software.rs:336-346). */
+rt_status rt_object_box(rt_layout layout, const rt_blas* blas, const float* positions, const uint32_t* indices,
+                        uint32_t n_indices, float box[6]);
+/* Moved instances, on the host: every instance's record gets its new rows and world box (the
+ * packer's arithmetic over mesh_boxes[instances[i].mesh], 6 floats a mesh), the top level is
+ * refit over the new boxes with header word 3 counting refits, and rebuilt once 64 refits have
+ * been made (instance_bvh::place for a moved set), and reflection scene bounds are recomputed.
+ * The instances are the scene's, in record order, none singular; the rest of each record stays.
+ * rt_scene_move_instances does the same on the device. */
+rt_status rt_move_instances_host(rt_layout layout, uint32_t* words, size_t n_words, const rt_instance* instances,
+                                 uint32_t n, const float* mesh_boxes, uint32_t n_meshes);
+/* The same on an uploaded scene, on the device (records, top-level refit one launch per height,
+ * scene bounds), with rt_move_instances_host's words bit for bit: the per-frame instance update
+ * of the reference (instance_words + instance_bvh::place, src/instance_bvh.rs:162-275) without a
+ * host round trip. Host arrays; it reads the scene's header and, on the first call and after each
+ * rebuild, the top level's topology, synchronously. */
+rt_status rt_scene_move_instances(rt_ctx* ctx, rt_scene* scene, const rt_instance* instances, uint32_t n,
+                                  const float* mesh_boxes, uint32_t n_meshes, void* stream);
+
 /* Instance top level alone (instance_bvh.rs:346-366): boxes are 6 floats (lo xyz, hi xyz).
  * Call with out NULL to learn the size. */
 rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);

@@ -104,7 +104,8 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
-           "rt_trace_static", "rt_scene_wide8_depth", "rt_wide8_check", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
+           "rt_trace_static", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
+           "rt_scene_move_instances", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
            "rt_rnf_placement_get", "rt_rnf_encode", "rt_rnf_pack_gi", "rt_rnf_world", "rt_rnf_free")
@@ -138,6 +139,11 @@ def lib() -> ctypes.CDLL:
     L.rt_scene_prepare.argtypes = [_vp, _vp, ctypes.c_int]
     L.rt_scene_wide8_depth.argtypes = [_vp, _u32p]
     L.rt_wide8_check.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, _u32p, ctypes.c_char_p, ctypes.c_size_t]
+    L.rt_object_box.argtypes = [ctypes.c_int, _vp, _f32p, _u32p, ctypes.c_uint32, _f32p]
+    L.rt_move_instances_host.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, ctypes.POINTER(RtInstance),
+                                         ctypes.c_uint32, _f32p, ctypes.c_uint32]
+    L.rt_scene_move_instances.argtypes = [_vp, _vp, ctypes.POINTER(RtInstance), ctypes.c_uint32, _f32p,
+                                          ctypes.c_uint32, _vp]
     L.rt_scene_device_bytes.argtypes = [_vp]
     L.rt_scene_device_bytes.restype = ctypes.c_size_t
     L.rt_trace.argtypes = [_vp, _vp, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
@@ -316,6 +322,30 @@ def pack_scene(layout: int, meshes, instances, tlas_mode: int = -1, primitives=N
     return out
 
 
+def object_boxes(layout: int, meshes) -> np.ndarray:
+    """(n_meshes, 6) float32: the object box rt_pack_scene places for each mesh (Blas objects)."""
+    out = np.zeros((len(meshes), 6), np.float32)
+    for m, b in enumerate(meshes):
+        st = lib().rt_object_box(layout, b.h, _np_ptr(b.positions, _f32p), _np_ptr(b.indices, _u32p),
+                                 len(b.indices), _np_ptr(out[m], _f32p))
+        if st != 0:
+            raise RtError(st, "object box")
+    return out
+
+
+def move_instances_host(layout: int, words, instances, mesh_boxes) -> np.ndarray:
+    """A copy of packed words with `instances` (Instances-like, the scene's, in order) moved: new
+    records, the top level refit (or rebuilt after 64 refits) and scene bounds
+    (rt_move_instances_host)."""
+    w = np.array(words, np.uint32, copy=True)
+    arr, n = _instance_array(layout, instances)
+    boxes = np.ascontiguousarray(mesh_boxes, np.float32).reshape(-1, 6)
+    st = lib().rt_move_instances_host(layout, _np_ptr(w, _u32p), len(w), arr, n, _np_ptr(boxes, _f32p), len(boxes))
+    if st != 0:
+        raise RtError(st, "moved instances refused (count, mesh index or a singular placement)")
+    return w
+
+
 def wide8_check(layout: int, words) -> dict:
     """Builds the 8-wide layout on the host and checks it (rt_wide8_check); raises RtError(LAYOUT)
     with the reason, else returns its node, triangle, depth and BLAS counts."""
@@ -382,6 +412,18 @@ class Scene:
     def prepare(self, kernel: str = "wide8"):
         """Build the derived layout `kernel` reads (the 8-wide BVH for "wide8")."""
         self.engine._check(lib().rt_scene_prepare(self.engine.ctx, self.handle, KERNELS[kernel]))
+
+    def move_instances(self, instances, mesh_boxes, stream=None):
+        """Moves the scene's instances on the device (rt_scene_move_instances); `instances` as
+        pack_scene takes them (the scene's, in order), `mesh_boxes` from object_boxes()."""
+        arr, n = _instance_array(self.layout, instances)
+        boxes = np.ascontiguousarray(mesh_boxes, np.float32).reshape(-1, 6)
+        if stream is None:
+            import torch
+            stream = torch.cuda.current_stream().cuda_stream
+        s = stream
+        self.engine._check(lib().rt_scene_move_instances(self.engine.ctx, self.handle, arr, n, _np_ptr(boxes, _f32p),
+                                                         len(boxes), s))
 
     def wide8_depth(self) -> int:
         """Levels of the deepest 8-wide BLAS (after prepare("wide8")); the shared stack takes 16."""

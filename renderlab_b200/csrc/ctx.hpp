@@ -36,6 +36,12 @@ struct rt_scene {
   size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
   uint32_t w8_depth = 0;  // levels of the deepest 8-wide BLAS
   std::map<uint32_t, RefitLevels> refit;  // by the BLAS's node base word
+  // rt_scene_move_instances: staging for the moved instances and mesh boxes, and the top level's
+  // nodes grouped by height (deepest last), kept until a rebuild changes the tree.
+  void* d_move = nullptr;
+  size_t move_bytes = 0;
+  std::vector<uint32_t> top_order, top_level_start;
+  uint32_t* d_top_order = nullptr;
 };
 
 struct rt_blas {

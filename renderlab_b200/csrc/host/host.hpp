@@ -92,6 +92,19 @@ bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& i
              std::vector<uint32_t>& out, std::string& err);
 bool pack_reflection(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst,
                      int tlas_mode, std::vector<uint32_t>& out, std::string& err);
+// Instances moved in packed words (pack.cpp): each record's rows and world box rewritten with
+// the packer's arithmetic (mesh_boxes: the object box the packer used for each mesh), then the
+// top level as instance_bvh::place treats a moved set: refit (word 3 counting refits) until
+// TLAS_REFITS refits, then rebuilt; reflection scene bounds recomputed. Every instance must be
+// non-singular and the count unchanged.
+constexpr uint32_t TLAS_REFITS = 64;  // instance_bvh.rs:94
+bool move_instances(uint32_t layout, uint32_t* words, size_t n_words, const std::vector<Placement>& inst,
+                    const std::vector<Aabb>& mesh_boxes, std::string& err);
+// A placement the packers skip or refuse: a zero determinant or a non-finite row (pack.cpp).
+bool is_singular(const Placement& g);
+// The world box (with the layout's margin) of a placement of an object box (pack.cpp), as the
+// packers write instance words 12-17.
+void instance_box(uint32_t layout, const float* model, const Aabb& obj, float lo[3], float hi[3]);
 
 // Cooked files (cooked.cpp). RLB: crates/asset/src/cluster_bvh/codec.rs; RNF:
 // crates/asset/src/near_field.rs:540-660. A BLAS is written as the near-field builder's cluster

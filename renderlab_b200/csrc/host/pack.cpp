@@ -27,6 +27,8 @@ void to_world(const float* m, const float* p, float* out) {
   }
 }
 
+}  // namespace
+
 bool is_singular(const Placement& g) {
   const float* m = g.model;
   double det = (double)m[0] * ((double)m[5] * m[10] - (double)m[6] * m[9]) -
@@ -37,6 +39,8 @@ bool is_singular(const Placement& g) {
     if (!std::isfinite(r)) return true;
   return false;
 }
+
+namespace {
 
 struct TriKey {
   uint32_t a, b, c;
@@ -100,6 +104,65 @@ uint32_t near_base(const float* model, const std::vector<NearMasks>& near, const
 
 }  // namespace
 
+void instance_box(uint32_t layout, const float* model, const Aabb& obj, float lo[3], float hi[3]) {
+  Aabb wb;
+  world_box(model, obj, wb);
+  if (layout == 0) {  // gi_bvh.rs:236-262: a pad per axis
+    for (int a = 0; a < 3; ++a) {
+      const float pad = 1e-5f * (1.0f + hi_of(std::fabs(wb.lo[a]), std::fabs(wb.hi[a])));
+      lo[a] = wb.lo[a] - pad, hi[a] = wb.hi[a] + pad;
+    }
+    return;
+  }
+  // world_bounds (reflection_software.rs:373-388): one margin from the largest coordinate or
+  // extent over the three axes.
+  float margin = 0.0f;
+  for (int a = 0; a < 3; ++a)
+    margin = hi_of(margin, hi_of(hi_of(std::fabs(wb.hi[a]), std::fabs(wb.lo[a])), wb.hi[a] - wb.lo[a]));
+  margin = margin * 1e-5f;
+  for (int a = 0; a < 3; ++a) lo[a] = wb.lo[a] - margin, hi[a] = wb.hi[a] + margin;
+}
+
+bool move_instances(uint32_t layout, uint32_t* w, size_t n_words, const std::vector<Placement>& inst,
+                    const std::vector<Aabb>& mesh_boxes, std::string& err) {
+  const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
+  const uint32_t count = w[0];
+  if (inst.size() != count || (layout == 0 && w[4] > count))  // GI word 4: a see-through tail
+    return err = "moved instances must be the scene's instances, in record order", false;
+  if (header + stride * (size_t)count > n_words) return err = "instance records exceed the words", false;
+  std::vector<Aabb> boxes(count);
+  for (uint32_t i = 0; i < count; ++i) {
+    const Placement& g = inst[i];
+    if (g.mesh >= mesh_boxes.size()) return err = "instance mesh index out of range", false;
+    if (is_singular(g)) return err = "a moved instance is singular", false;
+    uint32_t* r = w + header + stride * (size_t)i;
+    for (int k = 0; k < 12; ++k) r[k] = as_bits(g.rows[k]);
+    instance_box(layout, g.model, mesh_boxes[g.mesh], boxes[i].lo, boxes[i].hi);
+    for (int a = 0; a < 3; ++a) r[12 + a] = as_bits(boxes[i].lo[a]), r[15 + a] = as_bits(boxes[i].hi[a]);
+  }
+  const size_t base = layout == 0 ? w[1] : (w[1] & ~3u);
+  if (w[1] != 0 && count >= 2) {  // instance_bvh::place, a moved set (the same records, new boxes)
+    if (base + tlas_reserve(count) > n_words) return err = "top level exceeds the words", false;
+    if (w[3] < TLAS_REFITS) {
+      w[3] += 1;
+      tlas_refit(w + base, boxes);
+    } else {
+      std::vector<uint32_t> nodes = tlas_build(boxes, true);
+      std::fill(w + base, w + base + tlas_reserve(count), 0u);
+      std::copy(nodes.begin(), nodes.end(), w + base);
+      w[3] = 0;
+    }
+  }
+  if (layout == 1) {  // finish_scene_bounds (reflection_software.rs:295-313)
+    Aabb scene = Aabb::empty();
+    for (const Aabb& b : boxes) scene.grow(b);
+    const size_t at = w[4];
+    if (at + 8 > n_words) return err = "scene bounds exceed the words", false;
+    for (int a = 0; a < 3; ++a) w[at + a] = as_bits(scene.lo[a]), w[at + 4 + a] = as_bits(scene.hi[a]);
+  }
+  return true;
+}
+
 bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& inst, int tlas_mode,
              std::vector<uint32_t>& out, std::string& err) {
   const size_t n = inst.size();
@@ -141,13 +204,9 @@ bool pack_gi(const std::vector<MeshRef>& meshes, const std::vector<Placement>& i
     const Blas& b = *meshes[g.mesh].blas;
     uint32_t* r = &head[16 + 32 * i];
     for (int k = 0; k < 12; ++k) r[k] = as_bits(g.rows[k]);
-    Aabb wb;
-    world_box(g.model, b.bounds, wb);
-    for (int a = 0; a < 3; ++a) {
-      float pad = 1e-5f * (1.0f + hi_of(std::fabs(wb.lo[a]), std::fabs(wb.hi[a])));
-      r[12 + a] = as_bits(wb.lo[a] - pad);
-      r[15 + a] = as_bits(wb.hi[a] + pad);
-    }
+    float lo[3], hi[3];
+    instance_box(0, g.model, b.bounds, lo, hi);
+    for (int a = 0; a < 3; ++a) r[12 + a] = as_bits(lo[a]), r[15 + a] = as_bits(hi[a]);
     for (int k = 0; k < 4; ++k) r[18 + k] = base[g.mesh][k];
     r[22] = b.root;
     r[23] = meshes[g.mesh].near.empty() ? g.near_base : near_base(g.model, meshes[g.mesh].near, near[g.mesh]);
@@ -243,16 +302,10 @@ bool pack_reflection(const std::vector<MeshRef>& meshes, const std::vector<Place
     }
     if (is_singular(g)) continue;
     for (int k = 0; k < 12; ++k) head.push_back(as_bits(g.rows[k]));
-    Aabb wb;
-    world_box(g.model, obj[g.mesh], wb);
-    // world_bounds (reflection_software.rs:373-388): one margin from the largest coordinate or
-    // extent over the three axes.
-    float margin = 0.0f;
-    for (int a = 0; a < 3; ++a)
-      margin = hi_of(margin, hi_of(hi_of(std::fabs(wb.hi[a]), std::fabs(wb.lo[a])), wb.hi[a] - wb.lo[a]));
-    margin = margin * 1e-5f;
-    for (int a = 0; a < 3; ++a) head.push_back(as_bits(wb.lo[a] - margin));
-    for (int a = 0; a < 3; ++a) head.push_back(as_bits(wb.hi[a] + margin));
+    float lo[3], hi[3];
+    instance_box(1, g.model, obj[g.mesh], lo, hi);
+    for (int a = 0; a < 3; ++a) head.push_back(as_bits(lo[a]));
+    for (int a = 0; a < 3; ++a) head.push_back(as_bits(hi[a]));
     head.push_back(base[g.mesh][0]);
     head.push_back(base[g.mesh][1]);
     head.push_back(roots[g.mesh]);

@@ -282,6 +282,8 @@ rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene) {
   cudaSetDevice(ctx->device);
   cudaFree(scene->d_words);
   cudaFree(scene->d_wide8);
+  cudaFree(scene->d_move);
+  cudaFree(scene->d_top_order);
   for (auto& kv : scene->refit) cudaFree(kv.second.d_order);
   ctx->scene_bytes -= scene->device_bytes;
   delete scene;
@@ -524,6 +526,48 @@ rt_status rt_pack_scene(rt_layout layout, const rt_blas* const* meshes, uint32_t
   std::copy(words.begin(), words.end(), out_words);
   *n_words = words.size();
   return RT_OK;
+}
+
+rt_status rt_object_box(rt_layout layout, const rt_blas* blas, const float* positions, const uint32_t* indices,
+                        uint32_t n_indices, float box[6]) {
+  if (!blas || !box || (unsigned)layout > 1u) return RT_ERR_INVALID_ARG;
+  rtb::Aabb b = rtb::Aabb::empty();
+  if (layout == RT_LAYOUT_GI) {
+    b = blas->b.bounds;
+  } else {
+    if (n_indices && (!positions || !indices)) return RT_ERR_INVALID_ARG;
+    for (uint32_t k = 0; k < n_indices; ++k) b.grow(positions + 3 * (size_t)indices[k]);
+  }
+  for (int a = 0; a < 3; ++a) box[a] = b.lo[a], box[3 + a] = b.hi[a];
+  return RT_OK;
+}
+
+namespace {
+bool placements_of(const rt_instance* instances, uint32_t n, std::vector<rtb::Placement>& out) {
+  if (n && !instances) return false;
+  out.resize(n);
+  for (uint32_t i = 0; i < n; ++i) {
+    const rt_instance& s = instances[i];
+    rtb::Placement& p = out[i];
+    std::copy(s.model, s.model + 12, p.model);
+    std::copy(s.rows, s.rows + 12, p.rows);
+    p.mesh = s.mesh, p.slot = s.slot, p.casts_shadow = s.casts_shadow, p.near_base = s.near_base;
+    std::copy(s.extra, s.extra + 8, p.extra);
+  }
+  return true;
+}
+}  // namespace
+
+rt_status rt_move_instances_host(rt_layout layout, uint32_t* words, size_t n_words, const rt_instance* instances,
+                                 uint32_t n, const float* mesh_boxes, uint32_t n_meshes) {
+  if (!words || n_words < 8 || (unsigned)layout > 1u || (n_meshes && !mesh_boxes)) return RT_ERR_INVALID_ARG;
+  std::vector<rtb::Placement> inst;
+  if (!placements_of(instances, n, inst)) return RT_ERR_INVALID_ARG;
+  std::vector<rtb::Aabb> boxes(n_meshes);
+  for (uint32_t m = 0; m < n_meshes; ++m)
+    for (int a = 0; a < 3; ++a) boxes[m].lo[a] = mesh_boxes[6 * m + a], boxes[m].hi[a] = mesh_boxes[6 * m + 3 + a];
+  std::string err;
+  return rtb::move_instances((uint32_t)layout, words, n_words, inst, boxes, err) ? RT_OK : RT_ERR_LAYOUT;
 }
 
 rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words) {

@@ -1,0 +1,46 @@
+"""Moving instances on the device (rt_scene_move_instances): the scene's words equal the host
+move's (rt_move_instances_host), bit for bit, over moves in a row (the top level refit each time,
+header word 3 counting) and across the rebuild after 64 refits; and traced rays see the moved
+scene as the oracle does."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from renderlab_b200 import api as A
+
+from . import helpers as H
+from .test_move_instances import _placements, _scene
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_device_move_equals_the_host_move(engine, layout):
+    import torch
+    meshes, inst = _scene(layout, n=64, seed=4)
+    words = A.pack_scene(layout, meshes, inst)
+    boxes = A.object_boxes(layout, meshes)
+    scene = engine.upload(layout, words)
+    try:
+        host = words
+        rng = np.random.default_rng(21)
+        for step in range(3):
+            new = _placements(len(inst), rng)
+            new.mesh = inst.mesh.copy()
+            if step == 2:  # the refit count at its limit: the next move rebuilds the top level
+                host = host.copy()
+                host[3] = 64
+                scene.update_records(host[:8])
+            host = A.move_instances_host(layout, host, new, boxes)
+            scene.move_instances(new, boxes)
+            torch.cuda.synchronize()
+            dev = scene.words()
+            assert np.array_equal(dev, host), f"move {step}: {int((dev != host).sum())} words differ"
+        # rays through the moved scene: the oracle's hits over the host-moved words
+        rays = H.random_rays(20_000, -120.0, 120.0, seed=8, tmax=500.0)
+        got = engine.trace(scene, torch.from_numpy(rays).cuda(), A.CLOSEST, "fast").cpu().numpy().view(np.uint32)
+        want = (O.gi_trace(host, rays, 0) if layout == A.LAYOUT_GI else O.rs_trace(host, rays, False))[0]
+        assert np.array_equal(got.reshape(want.shape), want)
+        assert (want[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)).any()
+    finally:
+        scene.release()
