@@ -351,6 +351,12 @@ rt_status rt_trace_static(rt_layout layout, const uint32_t* d_words, size_t n_wo
 #define RT_BUILD_MEDIAN 1u /* build_bvh (near_field.rs:172) */
 rt_status rt_blas_build(const float* positions, uint32_t n_positions, const uint32_t* indices,
                         uint32_t n_indices, uint32_t build_flags, rt_blas** out);
+/* The same build on the context's device (binned SAH or median splits level by level, node
+ * boxes quantised bottom-up on the device): host arrays in, a host BLAS out whose nodes, leaves,
+ * indices and leaf sources equal rt_blas_build's word for word, including the median rebuild of
+ * an SAH tree past 15 node levels. At most 2^29 triangles. Synchronous. */
+rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_positions, const uint32_t* indices,
+                               uint32_t n_indices, uint32_t build_flags, rt_blas** out);
 /* info: nodes, leaves, positions, indices, root, depth */
 rt_status rt_blas_info(const rt_blas* blas, uint32_t info[6]);
 /* The 16-word runtime node records (gi_bvh.rs:191-203), 16 * nodes words. */

@@ -105,7 +105,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
            "rt_trace_static", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
-           "rt_scene_move_instances", "rt_blas_build", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
+           "rt_scene_move_instances", "rt_blas_build", "rt_blas_build_device", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
            "rt_rnf_placement_get", "rt_rnf_encode", "rt_rnf_pack_gi", "rt_rnf_world", "rt_rnf_free")
@@ -174,6 +174,8 @@ def lib() -> ctypes.CDLL:
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
     L.rt_blas_build.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_vp)]
+    L.rt_blas_build_device.argtypes = [_vp, _f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32,
+                                       ctypes.POINTER(_vp)]
     L.rt_blas_info.argtypes = [_vp, _u32p]
     L.rt_blas_nodes.argtypes = [_vp, _u32p]
     L.rt_blas_indices.argtypes = [_vp, _u32p]
@@ -228,6 +230,20 @@ class Blas:
         if st != 0:
             raise RtError(st, "BVH geometry needs a nonempty, finite triangle list")
         self.h = h
+
+    @classmethod
+    def build_device(cls, engine: "Engine", positions, indices, median: bool = False) -> "Blas":
+        """The same BLAS built on the engine's GPU (rt_blas_build_device): word for word the host
+        build's records."""
+        self = cls.__new__(cls)
+        self.positions = np.ascontiguousarray(positions, np.float32).reshape(-1, 3)
+        self.indices = np.ascontiguousarray(indices, np.uint32).reshape(-1)
+        h = _vp()
+        engine._check(lib().rt_blas_build_device(engine.ctx, _np_ptr(self.positions, _f32p), len(self.positions),
+                                                 _np_ptr(self.indices, _u32p), len(self.indices), 1 if median else 0,
+                                                 ctypes.byref(h)))
+        self.h = h
+        return self
 
     @classmethod
     def adopt(cls, h) -> "Blas":

@@ -51,3 +51,15 @@ def random_rays(n, lo, hi, seed=7, tmax=1e30):
     o = s.range(lo, hi, n, 3)
     d = s.unit_vectors(n)
     return S.pack_rays(o, d, 0.0, tmax)
+
+
+def deep_sah_mesh(n: int = 390):
+    """Triangles at exponentially spaced x (x_i = 1.25^(0.999 i)): binned SAH peels a few off the
+    far end at each split, so its tree passes 15 node levels and build_bvh_sah falls back to
+    median splits (near_field.rs:184-190)."""
+    x = np.power(np.float32(1.25), np.arange(n, dtype=np.float32) * np.float32(0.999)).astype(np.float32)
+    p = np.zeros((3 * n, 3), np.float32)
+    p[0::3, 0] = p[1::3, 0] = p[2::3, 0] = x
+    p[1::3, 1] = 1.0
+    p[2::3, 2] = 1.0
+    return p, np.arange(3 * n, dtype=np.uint32)
