@@ -67,6 +67,8 @@ def parse(argv=None):
     ap.add_argument("--small", action="store_true", help="a reduced workload (profiling captures)")
     ap.add_argument("--precision", type=int, default=-1,
                     help="rays checked against the FP64 oracle (default: 65,536 for --config 3, else 0)")
+    ap.add_argument("--blas-build", action="store_true",
+                    help="time the GPU BLAS build (rt_blas_build_device) against the host build on cluster meshes")
     return ap.parse_args(argv)
 
 
@@ -857,9 +859,44 @@ def run_ours(args):
     engine.close()
 
 
+def run_blas_build(args):
+    """One JSON line per mesh size (cluster soup of 0.25M, 1M and 4M triangles): the host SAH build
+    (rt_blas_build) once and the GPU build (rt_blas_build_device) --steps times after --warmup
+    (at most 10), each end to end from host arrays to a host BLAS, wall clock; the median GPU time;
+    and whether the two builds' records are equal."""
+    import time
+
+    from renderlab_b200 import api as A
+    from renderlab_b200 import scenes as S
+    engine = A.Engine(0)
+    steps = max(1, min(args.steps, 10))
+    for n in ((250_000,) if args.small else (250_000, 1_000_000, 4_000_000)):
+        m = S.clusters(n, config=2 if n < 4_000_000 else 3)
+        t = time.perf_counter()
+        host = A.Blas(m.positions, m.indices)
+        host_ms = (time.perf_counter() - t) * 1e3
+        for _ in range(args.warmup):
+            A.Blas.build_device(engine, m.positions, m.indices)
+        times = []
+        for _ in range(steps):
+            t = time.perf_counter()
+            dev = A.Blas.build_device(engine, m.positions, m.indices)
+            times.append((time.perf_counter() - t) * 1e3)
+        gpu_ms = float(np.median(times))
+        same = bool(np.array_equal(host.nodes(), dev.nodes()) and np.array_equal(host.bvh_indices(), dev.bvh_indices()))
+        print(json.dumps({"metric": "BLAS build, host arrays to host BLAS (SAH)", "triangles": n,
+                          "host_ms": round(host_ms, 1), "gpu_ms": round(gpu_ms, 1),
+                          "gpu_ms_range": [round(min(times), 1), round(max(times), 1)],
+                          "gpu_mtris_per_s": round(n / gpu_ms / 1e3, 1), "speedup": round(host_ms / gpu_ms, 1),
+                          "same_records": same, "steps": steps, "warmup": args.warmup}), flush=True)
+    engine.close()
+
+
 def main():
     args = parse()
-    if args.impl == "reference":
+    if args.blas_build:
+        run_blas_build(args)
+    elif args.impl == "reference":
         run_reference(args)
     elif args.config == 5:
         run_serving(args)

@@ -26,6 +26,7 @@
 
 #include <algorithm>
 #include <memory>
+#include <thread>
 #include <vector>
 
 #include "ctx.hpp"
@@ -141,6 +142,18 @@ __device__ Choice choose(const float* lo, const float* hi, const uint32_t* cnt, 
 
 __device__ __forceinline__ unsigned long long median_key(const float* cen, uint32_t t, int axis) {
   return (unsigned long long)okey(cen[3 * (size_t)t + axis]) << 32 | t;
+}
+
+// build_blas's geometry checks (near_field.rs:208-214) on the device: bit 0 an index past the
+// positions, bit 1 a position that is not finite.
+__global__ void k_validate(const float* __restrict__ pos, uint32_t n_floats, const uint32_t* __restrict__ idx,
+                           uint32_t n_idx, uint32_t n_pos, uint32_t* __restrict__ bad) {
+  uint32_t found = 0;
+  for (size_t k = blockIdx.x * (size_t)blockDim.x + threadIdx.x; k < (size_t)n_floats + n_idx; k += (size_t)gridDim.x * blockDim.x) {
+    if (k < n_floats) found |= isfinite(pos[k]) ? 0u : 2u;
+    else found |= idx[k - n_floats] >= n_pos ? 1u : 0u;
+  }
+  if (found) atomicOr(bad, found);
 }
 
 // Centroids (near_field.rs:216-226: the corners summed in order, then / 3), the triangles' boxes
@@ -608,6 +621,15 @@ class Arena {
   size_t size_ = 0, used_ = 0;
 };
 
+struct Joiner {  // joins its thread on every return path
+  std::thread t;
+  explicit Joiner(std::thread&& x) : t(std::move(x)) {}
+  ~Joiner() { join(); }
+  void join() {
+    if (t.joinable()) t.join();
+  }
+};
+
 struct StreamGuard {
   cudaStream_t s = nullptr;
   ~StreamGuard() {
@@ -625,16 +647,22 @@ rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_p
   *out = nullptr;
   // build_blas's checks (near_field.rs:208-214)
   if (n_indices == 0 || n_indices % 3 != 0) return fail(ctx, RT_ERR_INVALID_ARG, "BVH geometry needs a nonempty triangle list");
-  for (uint32_t k = 0; k < n_indices; ++k)
-    if (indices[k] >= n_positions) return fail(ctx, RT_ERR_INVALID_ARG, "BVH geometry has an invalid index or position");
-  for (size_t k = 0; k < 3 * (size_t)n_positions; ++k)
-    if (!std::isfinite(positions[k])) return fail(ctx, RT_ERR_INVALID_ARG, "BVH geometry has an invalid index or position");
   const uint32_t nt = n_indices / 3;
   if (nt > MAX_TRIANGLES) return fail(ctx, RT_ERR_INVALID_ARG, "the device build takes at most 2^29 triangles");
+  if ((size_t)n_positions * 3 > 0xffffffffu) return fail(ctx, RT_ERR_INVALID_ARG, "the device build takes at most 2^32 / 3 positions");
   bool sah = !(build_flags & RT_BUILD_MEDIAN);
 
   std::lock_guard<std::mutex> lock(ctx->mu);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  // The host BLAS's own copy of the positions and their bounds (every position, gi_bvh.rs:70),
+  // formed on a second host thread while the device builds.
+  auto blas = std::make_unique<rt_blas>();
+  rtb::Blas& B = blas->b;
+  Joiner host_part(std::thread([&B, positions, n_positions] {
+    B.positions.assign(positions, positions + 3 * (size_t)n_positions);
+    B.bounds = rtb::Aabb::empty();
+    for (uint32_t p = 0; p < n_positions; ++p) B.bounds.grow(positions + 3 * (size_t)p);
+  }));
   StreamGuard sg;
   RT_CUDA(ctx, cudaStreamCreateWithFlags(&sg.s, cudaStreamNonBlocking));
   cudaStream_t st = sg.s;
@@ -675,7 +703,7 @@ rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_p
   ar.plan<uint32_t>((size_t)nt + 1);  // leaf marks
   ar.plan<uint32_t>((size_t)nt + 1);  // leaf ranks
   ar.plan<uint32_t>(seg_cap);  // record id of each range
-  ar.plan<uint32_t>(4);        // counters
+  ar.plan<uint32_t>(4);        // counters and the validation flag
   ar.plan<char>(cub_bytes);
   if (ar.allocate() != cudaSuccess) {
     cudaGetLastError();
@@ -707,6 +735,12 @@ rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_p
 
   RT_CUDA(ctx, cudaMemcpyAsync(d_pos, positions, 12 * (size_t)n_positions, cudaMemcpyHostToDevice, st));
   RT_CUDA(ctx, cudaMemcpyAsync(d_idx, indices, 4 * (size_t)n_indices, cudaMemcpyHostToDevice, st));
+  RT_CUDA(ctx, cudaMemsetAsync(d_count, 0, 16, st));
+  k_validate<<<4 * 148, 256, 0, st>>>(d_pos, 3 * n_positions, d_idx, n_indices, n_positions, d_count);
+  uint32_t bad = 0;
+  RT_CUDA(ctx, cudaMemcpyAsync(&bad, d_count, 4, cudaMemcpyDeviceToHost, st));
+  RT_CUDA(ctx, cudaStreamSynchronize(st));
+  if (bad) return fail(ctx, RT_ERR_INVALID_ARG, "BVH geometry has an invalid index or position");
   k_prepare<<<blocks(nt, 256), 256, 0, st>>>(d_pos, d_idx, nt, d_cen, d_tbk, d_perm);
   RT_CUDA(ctx, cudaGetLastError());
 
@@ -868,11 +902,6 @@ rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_p
   }
   RT_CUDA(ctx, cudaGetLastError());
 
-  auto blas = std::make_unique<rt_blas>();
-  rtb::Blas& B = blas->b;
-  B.positions.assign(positions, positions + 3 * (size_t)n_positions);
-  B.bounds = rtb::Aabb::empty();
-  for (uint32_t p = 0; p < n_positions; ++p) B.bounds.grow(positions + 3 * (size_t)p);
   B.nodes.resize(16 * (size_t)n_nodes);
   B.leaves.resize(2 * (size_t)n_leaves);
   B.indices.resize(n_indices);
@@ -883,6 +912,7 @@ rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_p
   RT_CUDA(ctx, cudaMemcpyAsync(B.leaf_source.data(), d_leaf_source, 4 * (size_t)n_leaves, cudaMemcpyDeviceToHost, st));
   RT_CUDA(ctx, cudaStreamSynchronize(st));
   B.root = n_nodes ? n_nodes - 1 : LEAF;  // postorder puts the root last; a one-leaf mesh is leaf 0
+  host_part.join();
   *out = blas.release();
   return RT_OK;
 }
