@@ -405,11 +405,11 @@ rt_status rt_object_box(rt_layout layout, const rt_blas* blas, const float* posi
  * rt_scene_move_instances does the same on the device. */
 rt_status rt_move_instances_host(rt_layout layout, uint32_t* words, size_t n_words, const rt_instance* instances,
                                  uint32_t n, const float* mesh_boxes, uint32_t n_meshes);
-/* The same on an uploaded scene, on the device (records, top-level refit one launch per height,
- * scene bounds), with rt_move_instances_host's words bit for bit: the per-frame instance update
- * of the reference (instance_words + instance_bvh::place, src/instance_bvh.rs:162-275) without a
- * host round trip. Host arrays; it reads the scene's header and, on the first call and after each
- * rebuild, the top level's topology, synchronously. */
+/* The same on an uploaded scene, on the device (records, top-level refit one launch per level,
+ * the rebuild after 64 refits, scene bounds), with rt_move_instances_host's words bit for bit:
+ * the per-frame instance update of the reference (instance_words + instance_bvh::place,
+ * src/instance_bvh.rs:162-275) without a host round trip. Host arrays; it reads the scene's
+ * header and, on the first call, the top level's topology, synchronously. */
 rt_status rt_scene_move_instances(rt_ctx* ctx, rt_scene* scene, const rt_instance* instances, uint32_t n,
                                   const float* mesh_boxes, uint32_t n_meshes, void* stream);
 
@@ -417,6 +417,9 @@ rt_status rt_scene_move_instances(rt_ctx* ctx, rt_scene* scene, const rt_instanc
  * Call with out NULL to learn the size. */
 rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);
 rt_status rt_tlas_refit(uint32_t* nodes, size_t n_words, const float* boxes, uint32_t n);
+/* rt_tlas_build (SAH, with the median rebuild of a tree too deep for a 48-entry stack, or
+ * median) run on the context's device: host boxes in, the same node words out. Synchronous. */
+rt_status rt_tlas_build_device(rt_ctx* ctx, const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);
 
 /* The BLAS's positions (xyz a vertex, as given to rt_blas_build or decoded), 3 * positions floats. */
 rt_status rt_blas_positions(const rt_blas* blas, float* out);

@@ -106,7 +106,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
            "rt_trace_static", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
            "rt_scene_move_instances", "rt_blas_build", "rt_blas_build_device", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
-           "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_refit", "rt_blas_positions",
+           "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_build_device", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
            "rt_rnf_placement_get", "rt_rnf_encode", "rt_rnf_pack_gi", "rt_rnf_world", "rt_rnf_free")
 
@@ -186,6 +186,7 @@ def lib() -> ctypes.CDLL:
                                 ctypes.POINTER(_u32p), _u32p, _u32p, ctypes.POINTER(RtInstance), ctypes.c_uint32,
                                 ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
     L.rt_tlas_build.argtypes = [_f32p, ctypes.c_uint32, ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
+    L.rt_tlas_build_device.argtypes = [_vp, _f32p, ctypes.c_uint32, ctypes.c_int, _u32p, ctypes.POINTER(ctypes.c_size_t)]
     L.rt_tlas_refit.argtypes = [_u32p, ctypes.c_size_t, _f32p, ctypes.c_uint32]
     _sz = ctypes.POINTER(ctypes.c_size_t)
     L.rt_blas_positions.argtypes = [_vp, _f32p]
@@ -394,6 +395,16 @@ def tlas_build(boxes, sah: bool = True) -> np.ndarray:
     out = np.zeros(size.value, np.uint32)
     lib().rt_tlas_build(_np_ptr(b, _f32p), len(b), int(sah), _np_ptr(out, _u32p), ctypes.byref(size))
     return out
+
+
+def tlas_build_device(engine: "Engine", boxes, sah: bool = True) -> np.ndarray:
+    """tlas_build run on the engine's GPU (rt_tlas_build_device): the same node words."""
+    b = np.ascontiguousarray(boxes, np.float32).reshape(-1, 6)
+    out = np.zeros(max(len(b) - 1, 1) * 32, np.uint32)  # the reserve: at most n - 1 nodes
+    size = ctypes.c_size_t(out.size)
+    engine._check(lib().rt_tlas_build_device(engine.ctx, _np_ptr(b, _f32p), len(b), int(sah), _np_ptr(out, _u32p),
+                                             ctypes.byref(size)))
+    return out[: size.value]
 
 
 def tlas_refit(nodes, boxes) -> np.ndarray:

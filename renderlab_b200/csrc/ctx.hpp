@@ -83,6 +83,15 @@ struct rt_ctx {
 
 namespace rtc {
 
+// The instance top level built on the device (tlas_build.cu), word for word rtb::tlas_build's:
+// instance i's box is lo xyz at d_box_words[i * stride], hi xyz right after (float bits). The
+// nodes go to d_out (cap_words available, the rest zeroed); with d_order, the node ids grouped
+// by level, deepest first (a bottom-up refit order), level starts in *level_start. Synchronous
+// on `st`; the caller holds the context's lock.
+rt_status tlas_build_device(rt_ctx* ctx, const uint32_t* d_box_words, size_t stride, uint32_t n, bool sah, uint32_t* d_out,
+                            size_t cap_words, uint32_t* d_order, std::vector<uint32_t>* level_start, uint32_t* n_nodes,
+                            cudaStream_t st);
+
 constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BYTES = 32;
 #ifndef RT_HOST_CHUNK_LOG2
 #define RT_HOST_CHUNK_LOG2 19

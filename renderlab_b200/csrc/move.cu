@@ -1,7 +1,8 @@
 // Moving the instances of an uploaded scene on the device: the records' rows and world boxes
 // (the packers' arithmetic: gi_bvh.rs:230-274, reflection_software.rs:347-388), the top level
 // refit over the new boxes as instance_bvh::place does for a moved set (instance_bvh.rs:162-275:
-// refit, word 3 counting refits, a rebuild after 64), and the reflection layout's scene bounds
+// refit, word 3 counting refits, a rebuild after 64, made on the device by tlas_build.cu), and
+// the reflection layout's scene bounds
 // (reflection_software.rs:295-313). Every float operation is an explicit round-to-nearest step in
 // the host code's order, so the words equal rt_move_instances_host's, bit for bit.
 #include <cuda_runtime.h>
@@ -222,18 +223,26 @@ extern "C" rt_status rt_scene_move_instances(rt_ctx* ctx, rt_scene* scene, const
     if (base + span > scene->n_words) return fail(ctx, RT_ERR_LAYOUT, "top level exceeds the scene's words");
     uint32_t refits = head[3];
     std::vector<uint32_t> nodes;
-    if (refits >= rtb::TLAS_REFITS) {  // rebuilt, from the same boxes computed on the host
-      std::vector<rtb::Aabb> boxes(n);
-      std::vector<rtb::Aabb> obj(n_meshes);
-      for (uint32_t m = 0; m < n_meshes; ++m)
-        for (int a = 0; a < 3; ++a) obj[m].lo[a] = mesh_boxes[6 * m + a], obj[m].hi[a] = mesh_boxes[6 * m + 3 + a];
-      for (uint32_t i = 0; i < n; ++i) rtb::instance_box(layout, placed[i].model, obj[placed[i].mesh], boxes[i].lo, boxes[i].hi);
-      nodes = rtb::tlas_build(boxes, true);
-      nodes.resize(span, 0);
-      RT_CUDA(ctx, cudaMemcpyAsync(scene->d_words + base, nodes.data(), 4 * span, cudaMemcpyHostToDevice, s));
-      RT_CUDA(ctx, cudaStreamSynchronize(s));  // `nodes` leaves scope
-      refits = 0;
+    if (refits >= rtb::TLAS_REFITS) {
+      // Rebuilt on the device from the records' new boxes (instance_bvh::place for a moved set),
+      // with the new tree's refit order.
+      RT_CUDA(ctx, cudaFree(scene->d_top_order));
+      scene->d_top_order = nullptr;
       scene->top_order.clear();
+      if (cudaMalloc(&scene->d_top_order, 4 * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(ctx, RT_ERR_OOM, "top-level order");
+      }
+      const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
+      uint32_t n_nodes = 0;
+      std::vector<uint32_t> starts;
+      const rt_status st = tlas_build_device(ctx, scene->d_words + header + 12, stride, n, true, scene->d_words + base, span,
+                                             scene->d_top_order, &starts, &n_nodes, s);
+      if (st != RT_OK) return st;
+      scene->top_order.resize(n_nodes);
+      RT_CUDA(ctx, cudaMemcpy(scene->top_order.data(), scene->d_top_order, 4 * (size_t)n_nodes, cudaMemcpyDeviceToHost));
+      scene->top_level_start = starts;
+      refits = 0;
     } else {
       if (scene->top_order.empty()) {  // the tree's topology, once (and after every rebuild)
         nodes.resize(span);

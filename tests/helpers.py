@@ -63,3 +63,15 @@ def deep_sah_mesh(n: int = 390):
     p[1::3, 1] = 1.0
     p[2::3, 2] = 1.0
     return p, np.arange(3 * n, dtype=np.uint32)
+
+
+def deep_tlas_boxes(n: int = 400):
+    """Unit boxes at exponentially spaced x (x_i = 1.25^(i / 2)): instance_bvh's SAH peels a few off
+    the far end at each split, so past about 300 boxes the collapsed tree is too deep for a
+    48-entry stack and the build falls back to median splits (instance_bvh.rs:346-366)."""
+    x = np.power(np.float32(1.25), np.arange(n, dtype=np.float32) * np.float32(0.5)).astype(np.float32)
+    b = np.zeros((n, 6), np.float32)
+    b[:, 0], b[:, 3] = x - np.float32(0.5), x + np.float32(0.5)
+    b[:, 1] = b[:, 2] = np.float32(-0.5)
+    b[:, 4] = b[:, 5] = np.float32(0.5)
+    return b
