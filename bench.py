@@ -863,7 +863,8 @@ def run_blas_build(args):
     """One JSON line per mesh size (cluster soup of 0.25M, 1M and 4M triangles): the host SAH build
     (rt_blas_build) once and the GPU build (rt_blas_build_device) --steps times after --warmup
     (at most 10), each end to end from host arrays to a host BLAS, wall clock; the median GPU time;
-    and whether the two builds' records are equal."""
+    and whether the two builds' records are equal. Then the same for the instance top level
+    (rt_tlas_build against rt_tlas_build_device) at 10k and 100k instances."""
     import time
 
     from renderlab_b200 import api as A
@@ -889,6 +890,29 @@ def run_blas_build(args):
                           "gpu_ms_range": [round(min(times), 1), round(max(times), 1)],
                           "gpu_mtris_per_s": round(n / gpu_ms / 1e3, 1), "speedup": round(host_ms / gpu_ms, 1),
                           "same_records": same, "steps": steps, "warmup": args.warmup}), flush=True)
+    # The instance top level: host tlas_build against rt_tlas_build_device on random placements
+    # (centres uniform in [-500, 500]^3, half extents uniform in [0.5, 4]).
+    rng = np.random.default_rng(1)
+    for n in ((10_000,) if args.small else (10_000, 100_000)):
+        c = rng.uniform(-500, 500, (n, 3)).astype(np.float32)
+        h = rng.uniform(0.5, 4, (n, 3)).astype(np.float32)
+        boxes = np.concatenate([c - h, c + h], 1).astype(np.float32)
+        t = time.perf_counter()
+        want = A.tlas_build(boxes, True)
+        host_ms = (time.perf_counter() - t) * 1e3
+        for _ in range(args.warmup):
+            A.tlas_build_device(engine, boxes, True)
+        times = []
+        for _ in range(steps):
+            t = time.perf_counter()
+            got = A.tlas_build_device(engine, boxes, True)
+            times.append((time.perf_counter() - t) * 1e3)
+        gpu_ms = float(np.median(times))
+        print(json.dumps({"metric": "top-level build, host boxes to host words (SAH)", "instances": n,
+                          "host_ms": round(host_ms, 2), "gpu_ms": round(gpu_ms, 2),
+                          "gpu_ms_range": [round(min(times), 2), round(max(times), 2)],
+                          "speedup": round(host_ms / gpu_ms, 1), "same_words": bool(np.array_equal(want, got)),
+                          "steps": steps, "warmup": args.warmup}), flush=True)
     engine.close()
 
 
