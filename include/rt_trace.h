@@ -305,7 +305,7 @@ rt_status rt_server_destroy(rt_server* srv);
 
 /* Host-buffer form: copies rays in and hits out through the context's pinned staging and
  * device buffers (grown on first use, or sized ahead by rt_ctx_reserve), pipelined in chunks
- * over two streams. Returns when the hits are in h_hits. */
+ * over four streams. Returns when the hits are in h_hits. */
 rt_status rt_trace_host(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
                         const rt_ray* h_rays, void* h_hits, uint32_t n);
 /* Several host-buffer batches, each with its own mode and kernel, in one pipeline: the chunks of

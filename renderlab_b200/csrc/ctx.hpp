@@ -52,6 +52,13 @@ struct rt_rnf {
   rtb::Rnf f;
 };
 
+// Chunks a host-buffer call keeps in flight, each with its own stream and staging slot. A
+// stream runs its chunk's copy in, trace and copy out in order, so with two slots the next copy
+// in waits for the copy out two chunks back; four leave the copies off the critical path.
+#ifndef RT_HOST_STAGES
+#define RT_HOST_STAGES 4
+#endif
+
 struct rt_ctx {
   int device = 0;
   rtk::DevStatus* d_status = nullptr;
@@ -64,8 +71,8 @@ struct rt_ctx {
   std::mutex mu;
   std::string last_error;
   std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};
-  // rt_trace_host staging: two chunks in flight on two streams.
-  cudaStream_t streams[2] = {nullptr, nullptr};
+  // rt_trace_host staging: HOST_STAGES chunks in flight, one stream and staging slot each.
+  cudaStream_t streams[RT_HOST_STAGES] = {};
   void* d_rays = nullptr;
   void* d_hits = nullptr;
   size_t stage_rays = 0;  // rays per chunk buffer

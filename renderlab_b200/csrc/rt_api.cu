@@ -384,8 +384,8 @@ rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays) {
   cudaFree(ctx->d_hits);
   ctx->d_rays = ctx->d_hits = nullptr;
   ctx->stage_rays = 0;
-  if (cudaMalloc(&ctx->d_rays, 2 * want * RAY_BYTES) != cudaSuccess ||
-      cudaMalloc(&ctx->d_hits, 2 * want * GI_HIT_BYTES) != cudaSuccess) {
+  if (cudaMalloc(&ctx->d_rays, RT_HOST_STAGES * want * RAY_BYTES) != cudaSuccess ||
+      cudaMalloc(&ctx->d_hits, RT_HOST_STAGES * want * GI_HIT_BYTES) != cudaSuccess) {
     cudaGetLastError();
     return fail(ctx, RT_ERR_OOM, "staging allocation for %zu rays failed", want);
   }
@@ -410,13 +410,13 @@ rt_status rt_trace_host_batches(rt_ctx* ctx, const rt_scene* scene, const rt_hos
   std::lock_guard<std::mutex> lock(ctx->mu);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));
   const uint32_t chunk = (uint32_t)ctx->stage_rays;
-  uint32_t c = 0;  // chunks alternate between the two streams and staging halves across batches
+  uint32_t c = 0;  // chunks take the streams and staging slots in turn, across batches
   for (uint32_t k = 0; k < n_batches; ++k) {
     const rt_host_batch& hb = batches[k];
     const size_t bytes = hit_bytes(scene->layout, (uint32_t)hb.mode);
     for (uint32_t off = 0; off < hb.n; off += chunk, ++c) {
       const uint32_t m = std::min(chunk, hb.n - off);
-      const int b = c & 1;
+      const uint32_t b = c % RT_HOST_STAGES;
       cudaStream_t st = ctx->streams[b];
       char* dr = static_cast<char*>(ctx->d_rays) + (size_t)b * chunk * RAY_BYTES;
       char* dh = static_cast<char*>(ctx->d_hits) + (size_t)b * chunk * GI_HIT_BYTES;
