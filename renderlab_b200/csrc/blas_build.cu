@@ -31,6 +31,7 @@
 
 #include "ctx.hpp"
 #include "kernels/bvh4_quant.cuh"
+#include "kernels/order_keys.cuh"
 
 using namespace rtc;
 
@@ -67,17 +68,6 @@ struct LWork {  // a large range's reductions and decision
   int kind, axis, plane;
   uint32_t mid;
 };
-
-// Order-preserving keys of f32 (f32::total_cmp as an unsigned comparison), and back.
-__device__ __forceinline__ uint32_t okey(float f) {
-  const uint32_t b = __float_as_uint(f);
-  return b ^ ((b >> 31) ? 0xffffffffu : 0x80000000u);
-}
-__device__ __forceinline__ float unkey(uint32_t k) { return __uint_as_float(k ^ ((k >> 31) ? 0x80000000u : 0xffffffffu)); }
-__device__ __forceinline__ int32_t order_key(float f) {  // f32::total_cmp as a signed comparison
-  const int32_t x = __float_as_int(f);
-  return x ^ (int32_t)(((uint32_t)(x >> 31)) >> 1);
-}
 
 // The SAH bin of a centroid coordinate (near_field.rs:327-330): ((c - lo) / extent * 16) as
 // usize, at most 15.

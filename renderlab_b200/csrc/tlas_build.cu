@@ -21,7 +21,8 @@
 #include <vector>
 
 #include "ctx.hpp"
-#include "kernels/common.cuh"
+#include "kernels/bvh4_quant.cuh"
+#include "kernels/order_keys.cuh"
 
 using namespace rtc;
 
@@ -29,6 +30,11 @@ namespace {
 
 using rtk::EMPTY;
 using rtk::LEAF;
+using rtq::hi_of;
+using rtq::lo_of;
+using rtq::okey;
+using rtq::order_key;
+using rtq::unkey;
 
 constexpr uint32_t BINS = 16;         // instance_bvh.rs: BINS
 constexpr uint32_t NODE_WORDS = 32;
@@ -44,17 +50,6 @@ struct Seg {          // a range [b, e) of the instance permutation
   uint32_t pad;
 };
 
-__device__ __forceinline__ float lo_of(float a, float b) { return b < a ? b : a; }
-__device__ __forceinline__ float hi_of(float a, float b) { return b > a ? b : a; }
-__device__ __forceinline__ uint32_t okey(float f) {
-  const uint32_t b = __float_as_uint(f);
-  return b ^ ((b >> 31) ? 0xffffffffu : 0x80000000u);
-}
-__device__ __forceinline__ float unkey(uint32_t k) { return __uint_as_float(k ^ ((k >> 31) ? 0x80000000u : 0xffffffffu)); }
-__device__ __forceinline__ int32_t order_key(float f) {
-  const int32_t x = __float_as_int(f);
-  return x ^ (int32_t)(((uint32_t)(x >> 31)) >> 1);
-}
 __device__ __forceinline__ float area(const float* lo, const float* hi) {  // instance_bvh.rs:290-293
   const float e0 = hi_of(__fsub_rn(hi[0], lo[0]), 0.0f), e1 = hi_of(__fsub_rn(hi[1], lo[1]), 0.0f),
               e2 = hi_of(__fsub_rn(hi[2], lo[2]), 0.0f);
