@@ -1,7 +1,8 @@
 """Moving instances on the device (rt_scene_move_instances): the scene's words equal the host
 move's (rt_move_instances_host), bit for bit, over moves in a row (the top level refit each time,
-header word 3 counting) and across the rebuild after 64 refits; and traced rays see the moved
-scene as the oracle does."""
+header word 3 counting), across the rebuild after 64 refits (made on the device) and over the
+refits after it (in the rebuilt tree's level order); and traced rays see the moved scene as the
+oracle does."""
 import numpy as np
 import pytest
 
@@ -24,7 +25,7 @@ def test_device_move_equals_the_host_move(engine, layout):
     try:
         host = words
         rng = np.random.default_rng(21)
-        for step in range(3):
+        for step in range(5):
             new = _placements(len(inst), rng)
             new.mesh = inst.mesh.copy()
             if step == 2:  # the refit count at its limit: the next move rebuilds the top level
