@@ -35,6 +35,10 @@ def test_abi_version_and_null_arguments():
     assert lib.rt_blas_build(None, 0, None, 0, 0, None) == 1
     size = ctypes.c_size_t(0)
     assert lib.rt_tlas_build(None, 0, 1, None, ctypes.byref(size)) == 1
+    # the device builders and the device move refuse null arguments before touching a device
+    assert lib.rt_blas_build_device(None, None, 0, None, 0, 0, None) == 1
+    assert lib.rt_tlas_build_device(None, None, 0, 1, None, ctypes.byref(size)) == 1
+    assert lib.rt_scene_move_instances(None, None, None, 0, None, 0, None) == 1
 
 
 def test_context_without_device_reports_cuda_error():
