@@ -104,8 +104,9 @@ constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BY
 #define RT_HOST_CHUNK_LOG2 19
 #endif
 // Rays a host-buffer call stages per chunk (copies of one chunk overlap the next chunk's kernel).
-// 2^19: measured on the clusters-1M step against 2^20 (+2.6 % end to end: a shorter first copy
-// and last read-back) and 2^18 (-2.5 %: each launch's tail of idle lanes weighs more).
+// 2^19: measured end to end on the clusters-1M step with four stages at 804 Mrays/s, against 790
+// for 2^20 (a longer first copy and last read-back) and 777 for 2^18 (775 with eight stages: each
+// launch's tail of idle lanes weighs more).
 constexpr uint32_t HOST_CHUNK = 1u << RT_HOST_CHUNK_LOG2;
 constexpr uint32_t COUNTER_SLOTS = 4096;
 
