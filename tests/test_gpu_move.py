@@ -1,8 +1,8 @@
 """Moving instances on the device (rt_scene_move_instances): the scene's words equal the host
 move's (rt_move_instances_host), bit for bit, over moves in a row (the top level refit each time,
 header word 3 counting), across the rebuild after 64 refits (made on the device) and over the
-refits after it (in the rebuilt tree's level order); and traced rays see the moved scene as the
-oracle does."""
+refits after it (in the rebuilt tree's level order); traced rays see the moved scene as the
+oracle does; and the 8-wide walk, derived before the moves, finds the same triangles after them."""
 import numpy as np
 import pytest
 
@@ -22,6 +22,7 @@ def test_device_move_equals_the_host_move(engine, layout):
     words = A.pack_scene(layout, meshes, inst)
     boxes = A.object_boxes(layout, meshes)
     scene = engine.upload(layout, words)
+    scene.prepare("wide8")  # derived before the moves: they must not invalidate it
     try:
         host = words
         rng = np.random.default_rng(21)
@@ -43,5 +44,10 @@ def test_device_move_equals_the_host_move(engine, layout):
         want = (O.gi_trace(host, rays, 0) if layout == A.LAYOUT_GI else O.rs_trace(host, rays, False))[0]
         assert np.array_equal(got.reshape(want.shape), want)
         assert (want[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)).any()
+        # the 8-wide walk over the moved records and top level finds the same closest triangles
+        w8 = engine.trace(scene, torch.from_numpy(rays).cuda(), A.CLOSEST, "wide8").cpu().numpy().view(np.uint32)
+        ids = slice(1, 5) if layout == A.LAYOUT_GI else slice(1, 3)
+        same = (w8.reshape(want.shape)[:, ids] == want[:, ids]).all(axis=1)
+        assert same.mean() >= 0.999, same.mean()
     finally:
         scene.release()
