@@ -76,6 +76,9 @@ def lib():
                                           _u32p, _u64p]
         L.orc_gi_cell_rays.argtypes = [_u32p, ctypes.c_uint32, ctypes.c_int, _f32p]
         L.orc_gi_cell_rays.restype = None
+        L.orc_gi_light_rays.argtypes = [_u32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, _f32p,
+                                        ctypes.POINTER(ctypes.c_uint8)]
+        L.orc_gi_light_rays.restype = None
         L.orc_fp64_trace.argtypes = [_u32p, ctypes.c_int, _f32p, ctypes.c_uint32, ctypes.c_int, _f64p,
                                      _u32p, ctypes.c_int]
         _lib = L
@@ -261,6 +264,33 @@ def gi_cell_rays(cells, rotate=False):
     out = np.zeros((len(c) * 64, 8), np.float32)
     lib().orc_gi_cell_rays(_p(c, _u32p), len(c), int(bool(rotate)), _p(out, _f32p))
     return out
+
+
+def gi_light_rays(cells, lights):
+    """The GI cache's per-light visibility rays (gi_cache.wgsl gi_light / gi_light_direction /
+    gi_light_affects): cells (n, 8) uint32 records as gi_cell_rays takes them, lights (m, 20) uint32
+    80-byte light records. Returns (rays (n * m, 8) float32, affects (n, m) bool)."""
+    c = _c(cells, np.uint32).reshape(-1, 8)
+    lt = _c(lights, np.uint32).reshape(-1, 20)
+    rays = np.zeros((len(c) * len(lt), 8), np.float32)
+    affects = np.zeros((len(c), len(lt)), np.uint8)
+    lib().orc_gi_light_rays(_p(c, _u32p), len(c), _p(lt, _u32p), len(lt), _p(rays, _f32p),
+                            affects.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+    return rays, affects.astype(bool)
+
+
+def gi_light_bits(words, cells, lights, threads=None):
+    """gi_light's visibility words (gi_cache.wgsl:2054-2077) over a packed GI scene: per cell,
+    ceil(m / 32) uint32 words, bit l % 32 of word l // 32 set when light l reaches the cell and
+    gi_visible_within finds nothing in the way."""
+    rays, affects = gi_light_rays(cells, lights)
+    n, m = affects.shape
+    hits, _ = gi_trace(words, rays, 2, threads=threads)
+    visible = affects & (hits[:, 1] == 0xFFFFFFFF).reshape(n, m)
+    words_out = np.zeros((n, (m + 31) // 32), np.uint32)
+    for l in range(m):
+        words_out[:, l // 32] |= visible[:, l].astype(np.uint32) << np.uint32(l % 32)
+    return words_out
 
 
 def fp64_trace(words, rays, layout, any_hit=False, threads=None):
