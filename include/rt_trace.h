@@ -354,7 +354,8 @@ rt_status rt_blas_build(const float* positions, uint32_t n_positions, const uint
 /* The same build on the context's device (binned SAH or median splits level by level, node
  * boxes quantised bottom-up on the device): host arrays in, a host BLAS out whose nodes, leaves,
  * indices and leaf sources equal rt_blas_build's word for word, including the median rebuild of
- * an SAH tree past 15 node levels. At most 2^29 triangles. Synchronous. */
+ * an SAH tree past 15 node levels. At most 2^29 triangles. Synchronous, on a stream of its own;
+ * it holds the context's lock while it builds, so other calls on the same context wait. */
 rt_status rt_blas_build_device(rt_ctx* ctx, const float* positions, uint32_t n_positions, const uint32_t* indices,
                                uint32_t n_indices, uint32_t build_flags, rt_blas** out);
 /* info: nodes, leaves, positions, indices, root, depth */
@@ -418,7 +419,8 @@ rt_status rt_scene_move_instances(rt_ctx* ctx, rt_scene* scene, const rt_instanc
 rt_status rt_tlas_build(const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);
 rt_status rt_tlas_refit(uint32_t* nodes, size_t n_words, const float* boxes, uint32_t n);
 /* rt_tlas_build (SAH, with the median rebuild of a tree too deep for a 48-entry stack, or
- * median) run on the context's device: host boxes in, the same node words out. Synchronous. */
+ * median) run on the context's device: host boxes in, the same node words out. Synchronous, on a
+ * stream of its own; it holds the context's lock while it builds. */
 rt_status rt_tlas_build_device(rt_ctx* ctx, const float* boxes, uint32_t n, int sah, uint32_t* out, size_t* n_words);
 
 /* The BLAS's positions (xyz a vertex, as given to rt_blas_build or decoded), 3 * positions floats. */
