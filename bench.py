@@ -3,13 +3,17 @@ one JSON line on stdout.
 
 Workloads (seeded synthetic scenes and rays; splitmix64, seed 0x5EED0000 + config):
 
-* --config 2 (default) clusters-1M: 1,000,000 triangles in 2,000 clusters, reflection layout;
+* --config 3 (default) precision-4M: 4,000,000 cluster triangles (8,000 clusters of 500),
+  reflection layout; per step 16,777,216 mixed rays: 8,388,608 primary (4096 x 2048 pinhole),
+  5,033,164 cosine-hemisphere GI rays from the primary hits (closest hit) and 3,355,444 shadow
+  any-hit rays toward 16 point lights. It is the one workload that carries the metric whole:
+  closest and any-hit rays in one step, against the plain kernel at matched hits, with the FP64
+  report. The scene (about 200 MB of packed words) does not fit the 126 MB L2.
+* --config 2 clusters-1M: 1,000,000 triangles in 2,000 clusters, reflection layout;
   per step 4,194,304 coherent primary rays (2048 x 2048 pinhole from (0, 0, -250), fov 60 deg)
   plus 4,194,304 cosine-hemisphere GI rays spawned from the primary hits, closest hit.
 * --config 1 cubes-120k: 10,000 jittered unit cubes merged into one BLAS, GI layout; 1024 x 1024
   primaries closest hit plus one sun any-hit ray per hit.
-* --config 3 precision-4M: 4,000,000 cluster triangles; 16,777,216 mixed rays: 50 % primary
-  (4096 x 2048), 30 % GI hemisphere, 20 % shadow any-hit toward 16 point lights.
 * --config 4 batching: 64 BLAS (2k-500k triangles, log-uniform) under 10,000 randomly rotated,
   scaled and placed instances; 64 ray batches (1k-2M rays, log-uniform), closest / any hit.
 * --config 5 serving: 8 resident scenes (100k-8M triangles, BLAS + TLAS as config 4) under a
@@ -55,7 +59,7 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=60)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", type=int, default=2, choices=[1, 2, 3, 4, 5])
+    ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000", help="--config 5: Poisson arrival rates (req/s)")
     ap.add_argument("--requests", type=int, default=48, help="--config 5: requests per rate")
     ap.add_argument("--kernel", default="auto", help="auto: the autotuner's choice; or plain / fast / wide8")
@@ -66,7 +70,8 @@ def parse(argv=None):
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--small", action="store_true", help="a reduced workload (profiling captures)")
     ap.add_argument("--precision", type=int, default=-1,
-                    help="rays checked against the FP64 oracle (default: 65,536 for --config 3, else 0)")
+                    help="rays sampled for the FP64 check (default 65,536; 4,096 for --config 4), plus every ray "
+                         "where the product and the plain kernel differ; 0 skips the check")
     ap.add_argument("--blas-build", action="store_true",
                     help="time the GPU BLAS build (rt_blas_build_device) against the host build on cluster meshes")
     return ap.parse_args(argv)
@@ -355,44 +360,93 @@ def cpu_baseline_leg(wl: Workload, target_s: float, threads=None):
         (counts, [len(r) for r in sample])
 
 
-def precision_report(wl: Workload, results: dict, n_sample: int) -> dict:
-    """Hit identity and t of each arm's results against the FP64 oracle on a strided sample of
-    every batch, per batch. A near tie is a differing closest hit whose t lies within 1e-6
-    relative of the FP64 t; t errors are relative, over rays whose hit identity matches."""
+T_REL, TIE_REL, BARY_ABS = 1e-5, 1e-6, 1e-5
+
+
+def fp64_classify(layout: int, mode: int, got: np.ndarray, rays: np.ndarray, r64: np.ndarray, ident: np.ndarray):
+    """Each ray's result against the FP64 oracle's (r64 = [hit, t, u, v], ident). Returns
+    (status, t_rel, bary_abs): status 0 the same hit (identity, or the any-hit flag), 1 a near tie
+    (both hit, different identity, |t - t64| <= 1e-6 t64; any hit: the FP64 hit within 1e-5
+    relative of tmin or tmax), 2 unexplained. t_rel and bary_abs are NaN except where status is 0
+    and both hit: |t - t64| / t64 and max(|u - u64|, |v - v64|) (barycentrics range over [0, 1],
+    so their error is taken against that range)."""
+    ohit = r64[:, 0] > 0
+    n = len(got)
+    t_rel = np.full(n, np.nan)
+    bary = np.full(n, np.nan)
+    if mode:
+        ghit = got.reshape(n) != 0
+        t64 = r64[:, 1]
+        near = ohit & ((np.abs(t64 - rays[:, 7]) <= T_REL * np.abs(rays[:, 7]))
+                       | (np.abs(t64 - rays[:, 3]) <= T_REL * np.maximum(np.abs(rays[:, 3]), 1e-30)))
+        status = np.where(ghit == ohit, 0, np.where(near, 1, 2))
+        return status, t_rel, bary
+    cols, ocols, uv = (slice(1, 3), slice(2, 4), slice(3, 5)) if layout == 1 else (slice(1, 5), slice(2, 6), slice(5, 7))
+    ghit = got[:, 1] != (0 if layout == 1 else 0xFFFFFFFF)
+    t = got[:, 0].view(np.float32).astype(np.float64)
+    t64 = r64[:, 1]
+    both = ghit & ohit
+    same = both & (got[:, cols] == ident[:, ocols]).all(1)
+    m = (ghit != ohit) | (both & ~same)
+    tie = m & both & (np.abs(t - t64) <= TIE_REL * np.abs(t64))
+    status = np.where(~m, 0, np.where(tie, 1, 2))
+    t_rel[same] = np.abs(t[same] - t64[same]) / np.maximum(np.abs(t64[same]), 1e-30)
+    g_uv = got[:, uv].view(np.float32).astype(np.float64)
+    bary[same] = np.abs(g_uv[same] - r64[same, 2:4]).max(1)
+    return status, t_rel, bary
+
+
+def precision_report(wl: Workload, results: dict, n_sample: int, diff: list | None = None) -> dict:
+    """Each arm's results against the FP64 oracle, per batch, on a strided sample of every batch
+    plus (for the product arm) every ray where the product and the plain kernel disagree.
+
+    Per batch and arm: the sample's hit-identity mismatch rate, near ties and unexplained
+    mismatches; t error (relative) and barycentric error (absolute, on [0, 1]) over the sample's
+    matching hits, max and mean. For the product arm, `vs_plain` classifies every ray where the
+    two arms differ: the product agrees with FP64 (the plain kernel's f32 arithmetic erred), a
+    near tie, or unexplained."""
     from oracle import oracle as O
     frac = min(1.0, n_sample / max(1, wl.rays))
     idx = [np.arange(0, len(b.rays), max(1, int(round(1 / frac)))) if len(b.rays) else np.zeros(0, np.int64)
            for b in wl.batches]
-    ref = []
-    for b, ix in zip(wl.batches, idx):
-        ref.append(O.fp64_trace(wl.words, b.rays[ix], wl.layout, any_hit=b.mode != 0) if len(ix) else None)
+    diff = diff or [np.zeros(0, np.int64) for _ in wl.batches]
     out = {}
+    ref = []
+    for b, ix, dx in zip(wl.batches, idx, diff):
+        ids = np.union1d(ix, dx).astype(np.int64)
+        ref.append((ids, O.fp64_trace(wl.words, b.rays[ids], wl.layout, any_hit=b.mode != 0) if len(ids) else None))
     for arm, (hits, kernels) in results.items():
         per = {}
-        for b, ix, r, h, kern in zip(wl.batches, idx, ref, hits, kernels):
+        for b, ix, dx, (ids, r), h, kern in zip(wl.batches, idx, diff, ref, hits, kernels):
             if r is None:
                 continue
-            got = h[ix]
             r64, ident = r
-            ohit = r64[:, 0] > 0
-            if b.mode:
-                per[b.label] = dict(kernel=kern, any_rays=len(ix), flag_mismatches=int(((got != 0) != ohit).sum()))
-                continue
-            cols = slice(1, 3) if wl.layout == 1 else slice(1, 5)
-            ocols = slice(2, 4) if wl.layout == 1 else slice(2, 6)
-            ghit = got[:, 1] != (0 if wl.layout == 1 else 0xFFFFFFFF)
-            t = got[:, 0].view(np.float32).astype(np.float64)
-            t64 = r64[:, 1]
-            both = ghit & ohit
-            same = both & (got[:, cols] == ident[:, ocols]).all(1)
-            m = (ghit != ohit) | (both & ~same)
-            tie = m & both & (np.abs(t - t64) <= 1e-6 * np.abs(t64))
-            rel = np.abs(t[same] - t64[same]) / np.maximum(np.abs(t64[same]), 1e-30)
-            per[b.label] = dict(kernel=kern, closest_rays=len(ix), id_mismatch_rate=float(m.sum()) / max(1, len(ix)),
-                                near_ties=int(tie.sum()), other_mismatches=int((m & ~tie).sum()),
-                                t_rel_max=float(rel.max()) if len(rel) else 0.0,
-                                t_rel_mean=float(rel.mean()) if len(rel) else 0.0)
+            status, t_rel, bary = fp64_classify(wl.layout, b.mode, h[ids], b.rays[ids], r64, ident)
+            smp = np.isin(ids, ix)
+            st = status[smp]
+            rec = dict(kernel=kern, rays=int(smp.sum()), mismatch_rate=float((st != 0).mean()) if len(st) else 0.0,
+                       near_ties=int((st == 1).sum()), unexplained=int((st == 2).sum()))
+            if not b.mode:
+                tr, ba = t_rel[smp], bary[smp]
+                tr, ba = tr[~np.isnan(tr)], ba[~np.isnan(ba)]
+                rec.update(t_rel_max=float(tr.max()) if len(tr) else 0.0, t_rel_mean=float(tr.mean()) if len(tr) else 0.0,
+                           bary_abs_max=float(ba.max()) if len(ba) else 0.0,
+                           bary_abs_mean=float(ba.mean()) if len(ba) else 0.0)
+            if arm == "product":
+                dm = np.isin(ids, dx)
+                sd = status[dm]
+                rec["vs_plain"] = dict(differing=int(len(dx)), agrees_with_fp64=int((sd == 0).sum()),
+                                       near_ties=int((sd == 1).sum()), unexplained=int((sd == 2).sum()))
+            per[b.label] = rec
         out[arm] = per
+    tot = lambda arm, key: sum(v.get(key, 0) for v in out.get(arm, {}).values())
+    out["summary"] = dict(
+        product_unexplained=tot("product", "unexplained")
+        + sum(v["vs_plain"]["unexplained"] for v in out.get("product", {}).values() if "vs_plain" in v),
+        product_t_rel_max=max([v.get("t_rel_max", 0.0) for v in out.get("product", {}).values()] or [0.0]),
+        product_bary_abs_max=max([v.get("bary_abs_max", 0.0) for v in out.get("product", {}).values()] or [0.0]),
+        bar=f"ids equal except near ties (|dt| <= {TIE_REL:g} t); t within {T_REL:g} relative; "
+            f"barycentrics within {BARY_ABS:g}")
     return out
 
 
@@ -472,23 +526,43 @@ def run_reference(args):
 
     wl, _ = workload(args.config, holder, args.small, pack=oracle_pack, closest=cpu_closest)
     threads = os.cpu_count() or 1
+    # One strided sample of every batch, sized once from a probe so that a step is about
+    # min(20, 120 / steps) seconds of traversal; every step times the same sample.
     per_step = max(1.0, min(20.0, 120.0 / max(1, args.steps + args.warmup)))
-    steps = []
+    probe, _ = sample_of(wl, 4096)
+    t0 = time.perf_counter()
+    for b, r in zip(wl.batches, probe):
+        oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
+    per_ray = (time.perf_counter() - t0) / sum(len(r) for r in probe)
+    sample, frac = sample_of(wl, int(max(4096, per_step / max(per_ray, 1e-9))))
+    n = sum(len(r) for r in sample)
+    values, walls = [], []
     for k in range(args.warmup + args.steps):
-        base, _ = cpu_baseline_leg(wl, per_step, threads)
+        t0 = time.perf_counter()
+        for b, r in zip(wl.batches, sample):
+            oracle_trace(wl.words, wl.layout, r, b.mode, threads=threads)
+        wall = time.perf_counter() - t0
         if k >= args.warmup:
-            steps.append(base)
-    value = float(np.median([s["value"] for s in steps]))
-    cpu_line = dict(steps[-1])
-    cpu_line["value"] = value
+            values.append(n / wall / 1e6)
+            walls.append(wall)
+    value = float(np.median(values))
+    cpu_line = dict(value=value, unit=UNIT, cores=threads, kind="port",
+                    sample=f"{n:,} rays a step ({100 * frac:.2f} % of each batch of the step, strided), oracle "
+                           f"{'gi_traverse' if wl.layout == 0 else 'rs_trace'} (scalar f32 C++) on {threads} threads, "
+                           f"median {float(np.median(walls)):.2f} s a step")
     line = dict(metric=METRIC, value=value, unit=UNIT, impl="reference", n_gpus=world, steps=args.steps,
                 warmup=args.warmup, higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32",
-                data="synthetic", config=dict(workload=wl.name, layout="GI" if wl.layout == 0 else "reflection",
-                                              config=args.config),
+                data="synthetic", config=workload_config(wl, args.config),
                 cpu_baseline=cpu_line, e2e=dict(value=value, unit=UNIT, h2d_bytes_per_step=0, d2h_bytes_per_step=0),
                 ms_per_step=None, note="oracle restatement of the WGSL traversal loop on the host cores: the Rust/WGSL "
-                                       "reference cannot run here (no rustc, no Vulkan/wgpu)")
+                                       "reference cannot run here (no rustc, no Vulkan/wgpu); each step traces the "
+                                       "same strided sample of the step's rays")
     print(json.dumps(line), flush=True)
+
+
+def workload_config(wl: Workload, config: int) -> dict:
+    """The `config` object of the JSON line: the same on both arms for one workload."""
+    return dict(workload=wl.name, config=config, layout="GI" if wl.layout == 0 else "reflection")
 
 
 # ---------------------------------------------------------------- serving (config 5)
@@ -677,8 +751,10 @@ def run_ours(args):
         flush.zero_()
         product_step()
     torch.cuda.synchronize()
-    # matched hits: product results against the plain kernel's, per ray (ids, or the any-hit flag)
+    # matched hits: product results against the plain kernel's, per ray (ids, or the any-hit flag);
+    # the rays that differ go to the FP64 classification below
     matched, n_all = 0, 0
+    diff = [np.zeros(0, np.int64) for _ in wl.batches]
     for g, p in zip(wl.groups, plans):
         for j, i in enumerate(g):
             ref = plain_hits[i]
@@ -690,6 +766,7 @@ def run_ours(args):
                 same = got == ref
             matched += int(same.sum().item())
             n_all += ref.shape[0]
+            diff[i] = torch.nonzero(~same).flatten().cpu().numpy().astype(np.int64)
 
     bus = None
     try:
@@ -817,7 +894,7 @@ def run_ours(args):
         return 1 + (1 if p.desc["order"] != "none" else 0)
 
     launches_per_step = sum(launches(g, p) for g, p in zip(wl.groups, plans))
-    n_prec = args.precision if args.precision >= 0 else (65_536 if args.config == 3 else 0)
+    n_prec = args.precision if args.precision >= 0 else (4_096 if args.config == 4 else 65_536)
     precision = None
     if n_prec:
         prod = [None] * len(wl.batches)
@@ -830,14 +907,15 @@ def run_ours(args):
                 kern[i] = p.desc["kernel"] if p is not None else "plain"
         precision = precision_report(wl, {"product": (prod, kern),
                                           "plain": ([h.cpu().numpy().view(np.uint32) for h in plain_hits],
-                                                    ["plain"] * len(wl.batches))}, n_prec)
+                                                    ["plain"] * len(wl.batches))}, n_prec,
+                                     diff=[d[:100_000] for d in diff])
     line = dict(
         metric=METRIC, value=value, unit=UNIT, n_gpus=world, steps=args.steps, warmup=args.warmup, ms_per_step=ms,
         higher_is_better=True, scaling="weak", vs_baseline=None, dtype="f32", data="synthetic",
-        config=dict(workload=wl.name, config=args.config, layout="GI" if wl.layout == 0 else "reflection",
-                    triangles=wl.triangles, rays_per_step=n_step, l2="flushed before each step (256 MiB write)",
-                    parallelism=f"replicas x{world}", prepare_s=t_prep, tune_s=t_tune, **wl.info,
-                    plans=[p.desc if p is not None else {"kernel": "plain"} for p in plans]),
+        config=workload_config(wl, args.config),
+        workload_info=dict(triangles=wl.triangles, rays_per_step=n_step, l2="flushed before each step (256 MiB write)",
+                           parallelism=f"replicas x{world}", prepare_s=t_prep, tune_s=t_tune, **wl.info,
+                           plans=[p.desc if p is not None else {"kernel": "plain"} for p in plans]),
         plain=dict(value=plain_value, ms_per_step=ms_plain, launches_per_step=len(wl.batches)),
         speedup_vs_plain=value / plain_value,
         matched_hits_vs_plain=matched / max(1, n_all),

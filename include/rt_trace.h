@@ -338,12 +338,17 @@ rt_status rt_trace_counted(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_
  * counter and overflow count) is a static 256-byte device array that each GPU loading the
  * library holds until exit. d_words must be words rt_scene_validate accepted, copied to the
  * device by the caller (16-byte aligned); n is at most RT_STATIC_MAX_RAYS, larger batches are
- * refused with RT_ERR_INVALID_ARG. Hits are written as rt_trace writes them. The first call on
+ * refused with RT_ERR_INVALID_ARG, as are d_rays / d_words off a 16-byte boundary and d_hits off a
+ * 4-byte one. Hits are written as rt_trace writes them. The first call on
  * a device looks up the array's device address; make it before any stream capture. Every call
  * reuses (and first zeroes) the same array, so calls that overlap on the GPU race. */
 #define RT_STATIC_MAX_RAYS (1u << 31)
 rt_status rt_trace_static(rt_layout layout, const uint32_t* d_words, size_t n_words, rt_mode mode,
                           const rt_ray* d_rays, void* d_hits, uint32_t n, void* stream);
+/* The pushes the last rt_trace_static call on the current device dropped on a full traversal
+ * stack (its results may then miss hits), read from the same static array once `stream` has
+ * finished. The next rt_trace_static call on the device zeroes the count. Synchronous. */
+rt_status rt_trace_static_stack_drops(void* stream, uint64_t* out);
 
 /* ---- host builders (the CPU side of the path: crates/asset/src/near_field.rs:172-541,
  * src/instance_bvh.rs:162-460, src/gi_bvh.rs, src/reflection_software.rs) ---- */

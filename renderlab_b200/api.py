@@ -104,7 +104,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
-           "rt_trace_static", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
+           "rt_trace_static", "rt_trace_static_stack_drops", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
            "rt_scene_move_instances", "rt_blas_build", "rt_blas_build_device", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_build_device", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
@@ -171,6 +171,7 @@ def lib() -> ctypes.CDLL:
     L.rt_server_get_stats.argtypes = [_vp, ctypes.POINTER(RtServerStats), ctypes.c_int]
     L.rt_server_destroy.argtypes = [_vp]
     L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
+    L.rt_trace_static_stack_drops.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64)]
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
     L.rt_blas_build.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_vp)]
@@ -766,18 +767,45 @@ STATIC_MAX_RAYS = 1 << 31
 def trace_static(layout: int, d_words, rays, mode: int = CLOSEST, hits=None, stream=None):
     """rt_trace_static: the FAST traversal with no allocation by the library and no context.
 
-    d_words: the packed words in a caller-owned torch CUDA tensor (int32/uint32 view, words that
-    `validate` accepted); rays: (n, 8) float32 CUDA tensor. Returns the int32 hit tensor."""
+    d_words: the packed words in a caller-owned contiguous torch CUDA tensor (int32/uint32 view,
+    words that `validate` accepted); rays: a contiguous (n, 8) float32 CUDA tensor on the same
+    device. Returns the int32 hit tensor. The call runs with the rays' device current."""
     import torch
+    if rays.dtype != torch.float32 or rays.dim() != 2 or rays.shape[1] != 8 or not rays.is_contiguous():
+        raise ValueError("rays must be a contiguous (n, 8) float32 tensor")
+    if not rays.is_cuda or not d_words.is_cuda or d_words.device != rays.device:
+        raise ValueError("rays and d_words must be CUDA tensors on one device")
+    if d_words.element_size() != 4 or not d_words.is_contiguous():
+        raise ValueError("d_words must be a contiguous tensor of 32-bit words")
     n = rays.shape[0]
     words = hit_words(layout, mode)
+    shape = (n, words) if words > 1 else (n,)
     if hits is None:
-        hits = torch.empty((n, words) if words > 1 else (n,), dtype=torch.int32, device=rays.device)
-    s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
-    st = lib().rt_trace_static(layout, d_words.data_ptr(), d_words.numel(), mode, rays.data_ptr(), hits.data_ptr(), n, s)
+        hits = torch.empty(shape, dtype=torch.int32, device=rays.device)
+    elif (hits.device != rays.device or hits.element_size() != 4 or not hits.is_contiguous()
+          or hits.numel() != n * words):
+        raise ValueError(f"hits must be a contiguous tensor of {n * words} 32-bit words on the rays' device")
+    with torch.cuda.device(rays.device):
+        s = stream if stream is not None else torch.cuda.current_stream(rays.device).cuda_stream
+        st = lib().rt_trace_static(layout, d_words.data_ptr(), d_words.numel(), mode, rays.data_ptr(),
+                                   hits.data_ptr(), n, s)
     if st != 0:
         raise RtError(st, "rt_trace_static refused the call (sizes, alignment or layout)")
     return hits
+
+
+def trace_static_stack_drops(device=None, stream=None) -> int:
+    """rt_trace_static_stack_drops: pushes the last rt_trace_static call on `device` dropped on a
+    full stack (read after its stream has finished)."""
+    import torch
+    dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+    out = ctypes.c_uint64(0)
+    with torch.cuda.device(dev):
+        s = stream if stream is not None else torch.cuda.current_stream(dev).cuda_stream
+        st = lib().rt_trace_static_stack_drops(s, ctypes.byref(out))
+    if st != 0:
+        raise RtError(st, "rt_trace_static_stack_drops failed")
+    return int(out.value)
 
 
 # ---------------------------------------------------------------- the seam, batched

@@ -15,6 +15,13 @@
 //   re-intersected with the f64 Möller-Trumbore test over the source triangle in the packed
 //   words, in the exact arithmetic of the f64 reference (crates/asset/src/cluster_bvh/reference.rs:121-158), and ties resolve
 //   on (t, instance, triangle) as it does.
+// * Final values: a closest-hit walk records only the winner (t estimate, instance, 8-wide
+//   triangle); k_wide8_final then recomputes t, u, v of every hit in f64 over the source triangle
+//   (the same arithmetic), and the GI record's primitive words and normal, one thread per ray.
+//   f32 barycentrics of a ray whose origin lies hundreds of units from a sub-unit triangle carry
+//   errors near 1e-5 from the rounding of the coordinates alone; f64 leaves only the final
+//   rounding to f32. The pass is fully converged and coalesced, so it costs far less than the
+//   same work done by single lanes inside the divergent walk.
 #pragma once
 #include "plain.cuh"
 
@@ -48,7 +55,6 @@ struct W8View {
 struct W8Best {
   float t;          // f32 t of the best candidate (f32(t64) once re-tested)
   float band;       // bound on |t - t64| while !has64
-  float abs_err;    // its absolute (coordinate-rounding) part
   double t64;       // valid when has64
   bool has64;
   bool hit;
@@ -263,7 +269,6 @@ RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const 
     best.band = 0.0f;
   } else {
     best.hit = true, best.has64 = false, best.t = t, best.u = u, best.v = v, best.band = band;
-    best.abs_err = abs_err;
   }
   best.inst = inst, best.tri = tri, best.ident = ident;
   return AM == 2 ? lane_any : AM == 1;
@@ -445,6 +450,10 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   L.phase = 2;
 }
 
+// Ends a lane's ray. Any hit: the flag. Closest hit: the winner as the walk knows it -- the f32 t
+// estimate, the record's identity words and, in the words k_wide8_final overwrites, the instance
+// and 8-wide triangle that pass needs (reflection: u <- instance, v <- triangle; GI: word 2 <-
+// triangle). A miss is written in full here.
 template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, void* __restrict__ out,
                       unsigned long long* cnt) {
@@ -456,20 +465,14 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
     reinterpret_cast<uint32_t*>(out)[id] = b.hit ? 1u : 0u;
     return;
   }
-  if (b.hit && !b.has64 && b.abs_err > 2e-6f * b.t) {
-    w8_count<COUNT>(cnt, W8C_FINAL64);
-    // the f32 t is not within 1e-5 relative: report the f64 one
-    const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(V.tris) + 12 * (size_t)b.tri + 10);
-    double t64, u64, v64;
-    if (mt64<LAYOUT>(w, b.inst, ref, L.ray, t64, u64, v64)) b.t = (float)t64, b.u = (float)u64, b.v = (float)v64;
-  }
+  if (b.hit) w8_count<COUNT>(cnt, W8C_FINAL64);
   if (LAYOUT == 1) {
     uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * (size_t)id;
     o[0] = __float_as_uint(b.t);
     o[1] = b.hit ? ld(w, 8 + 24 * (size_t)b.inst + 21) + 1 : 0u;
     o[2] = b.hit ? b.ident : 0u;
-    o[3] = b.hit ? __float_as_uint(b.u) : 0u;
-    o[4] = b.hit ? __float_as_uint(b.v) : 0u;
+    o[3] = b.hit ? b.inst : 0u;
+    o[4] = b.hit ? b.tri : 0u;
     return;
   }
   uint32_t* o = reinterpret_cast<uint32_t*>(out) + 10 * (size_t)id;
@@ -478,8 +481,59 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
     o[5] = o[6] = 0, o[7] = o[8] = o[9] = 0;
     return;
   }
-  const size_t r = 16 + 32 * (size_t)b.inst;
-  const uint32_t ref = __ldg(reinterpret_cast<const uint32_t*>(V.tris) + 12 * (size_t)b.tri + 10);
+  o[0] = __float_as_uint(b.t), o[1] = b.inst, o[2] = b.tri;
+}
+
+// t, u, v of the f64 reference's Möller-Trumbore (reference.rs:121-158) over the source triangle
+// at word `ref`, without its range checks: the walk has already chosen this triangle. False only
+// when the f64 determinant is zero.
+template <uint32_t LAYOUT>
+__device__ __noinline__ bool mt64_values(const uint32_t* __restrict__ w, uint32_t inst, uint32_t ref, const Ray& ray,
+                                         double& t, double& u, double& v) {
+  D3 o, d;
+  ray64<LAYOUT>(w, inst, ray, o, d);
+  D3 a, ab, ac;
+  if (LAYOUT == 1) {
+    a = {ldf(w, ref), ldf(w, ref + 1), ldf(w, ref + 2)};
+    ab = {ldf(w, ref + 3), ldf(w, ref + 4), ldf(w, ref + 5)};
+    ac = {ldf(w, ref + 6), ldf(w, ref + 7), ldf(w, ref + 8)};
+  } else {
+    const size_t positions = ld(w, 16 + (size_t)inst * 32 + 20);
+    const uint32_t ia = ld(w, ref), ib = ld(w, ref + 1), ic = ld(w, ref + 2);
+    a = {ldf(w, positions + 3 * (size_t)ia), ldf(w, positions + 3 * (size_t)ia + 1), ldf(w, positions + 3 * (size_t)ia + 2)};
+    const D3 b = {ldf(w, positions + 3 * (size_t)ib), ldf(w, positions + 3 * (size_t)ib + 1), ldf(w, positions + 3 * (size_t)ib + 2)};
+    const D3 c = {ldf(w, positions + 3 * (size_t)ic), ldf(w, positions + 3 * (size_t)ic + 1), ldf(w, positions + 3 * (size_t)ic + 2)};
+    ab = dsub3(b, a);
+    ac = dsub3(c, a);
+  }
+  const D3 p = dcross(d, ac);
+  const double det = ddot(ab, p);
+  if (det == 0.0) return false;
+  const D3 s = dsub3(o, a);
+  const D3 q = dcross(s, ab);
+  u = __ddiv_rn(ddot(s, p), det);
+  v = __ddiv_rn(ddot(d, q), det);
+  t = __ddiv_rn(ddot(ac, q), det);
+  return true;
+}
+
+// The final values of one closest hit (see the header): f64 t, u, v; for the GI layout also the
+// primitive words and the world-space normal (unit_normal of the source winding, as gi_triangle's
+// caller forms it).
+template <uint32_t LAYOUT>
+RT_DEV void w8_final_hit(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t* __restrict__ o) {
+  if (LAYOUT == 1 ? o[1] == 0u : o[1] == EMPTY) return;  // a miss
+  const uint32_t inst = LAYOUT == 1 ? o[3] : o[1], tri = LAYOUT == 1 ? o[4] : o[2];
+  const uint4 q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
+  const uint32_t ident = q2.y, ref = q2.z;
+  double t64, u64, v64;
+  float t = __uint_as_float(o[0]), u = 0.0f, v = 0.0f;
+  if (mt64_values<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) t = (float)t64, u = (float)u64, v = (float)v64;
+  if (LAYOUT == 1) {
+    o[0] = __float_as_uint(t), o[3] = __float_as_uint(u), o[4] = __float_as_uint(v);
+    return;
+  }
+  const size_t r = 16 + 32 * (size_t)inst;
   const uint32_t prim_base = ld(w, r + 28), positions = ld(w, r + 20);
   const uint32_t ia = ld(w, ref), ib = ld(w, ref + 1), ic = ld(w, ref + 2);
   const F3 a = ld3(w, positions + 3 * (size_t)ia), bb = ld3(w, positions + 3 * (size_t)ib), c = ld3(w, positions + 3 * (size_t)ic);
@@ -489,11 +543,38 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
   const F3 nrm = unit_normal({add(add(mul(m0, cr.x), mul(m4, cr.y)), mul(m8, cr.z)),
                               add(add(mul(m1, cr.x), mul(m5, cr.y)), mul(m9, cr.z)),
                               add(add(mul(m2, cr.x), mul(m6, cr.y)), mul(m10, cr.z))});
-  o[0] = __float_as_uint(b.t), o[1] = b.inst;
-  if (prim_base != 0) o[2] = ld(w, prim_base + b.ident), o[3] = 0, o[4] = 0;
+  o[0] = __float_as_uint(t);
+  if (prim_base != 0) o[2] = ld(w, prim_base + ident), o[3] = 0, o[4] = 0;
   else o[2] = ia, o[3] = ib, o[4] = ic;
-  o[5] = __float_as_uint(b.u), o[6] = __float_as_uint(b.v);
+  o[5] = __float_as_uint(u), o[6] = __float_as_uint(v);
   o[7] = __float_as_uint(nrm.x), o[8] = __float_as_uint(nrm.y), o[9] = __float_as_uint(nrm.z);
+}
+
+// The final pass after a closest-hit WIDE8 launch: one thread per ray of the launch's ray space
+// (hits sit at the ray's index, whatever order the walk took the rays in); entries of a
+// many-batch launch that are any-hit queries are skipped.
+template <uint32_t LAYOUT>
+__global__ void __launch_bounds__(256) k_wide8_final(const uint32_t* __restrict__ w, W8View V, OneBatch src, uint32_t n) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t* o = reinterpret_cast<uint32_t*>(src.out) + (LAYOUT == 1 ? 5 : 10) * (size_t)i;
+  w8_final_hit<LAYOUT>(w, V, load_ray(src.rays, i), o);
+}
+template <uint32_t LAYOUT>
+__global__ void __launch_bounds__(256) k_wide8_final(const uint32_t* __restrict__ w, W8View V, ManyBatches src, uint32_t n) {
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= n) return;
+  uint32_t lo = 0, hi = src.entries;  // the last entry whose first ray is at or before g
+  while (hi - lo > 1) {
+    const uint32_t mid = (lo + hi) >> 1;
+    if (src.table[mid].first <= g) lo = mid;
+    else hi = mid;
+  }
+  const BatchEntry& e = src.table[lo];
+  if (e.mode != 0) return;
+  const uint32_t i = g - e.first;
+  uint32_t* o = reinterpret_cast<uint32_t*>(e.hits) + (LAYOUT == 1 ? 5 : 10) * (size_t)i;
+  w8_final_hit<LAYOUT>(w, V, load_ray(e.rays, i), o);
 }
 
 // Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
@@ -534,7 +615,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       L.ray = fetch(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
-      b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.abs_err = 0.0f, b.t64 = 0.0;
+      b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
       b.inst = EMPTY, b.tri = 0, b.ident = 0, b.u = b.v = 0.0f;
       L.phase = 1;
       L.flat = 0;
@@ -607,7 +688,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8_packet(const 
       L.ray = fetch(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
-      b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.abs_err = 0.0f, b.t64 = 0.0;
+      b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
       b.inst = EMPTY, b.tri = 0, b.ident = 0, b.u = b.v = 0.0f;
     }
     for (uint32_t i = 0; i < count && __any_sync(0xffffffffu, live); ++i) {

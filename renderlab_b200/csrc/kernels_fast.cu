@@ -1,6 +1,9 @@
 // Launchers for the FAST kernels: persistent grids sized to fill every SM once.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+
 #include "kernels/cells.cuh"
 #include "kernels/fast.cuh"
 #include "launch.hpp"
@@ -10,20 +13,30 @@ namespace rtl {
 namespace {
 constexpr int FAST_BLOCK = 128;
 
-// Resident blocks of `kernel` on the whole device, queried once per kernel (one device type).
+// Resident blocks of `kernel` on the current device, cached per (kernel, device) under a lock:
+// kernels of one signature share this template instance but can differ in registers, and
+// rt_trace_static calls arrive from any thread without a context lock.
 template <class K>
 cudaError_t resident_blocks(K kernel, uint32_t& out) {
-  static uint32_t cached = 0;
-  if (cached) {
-    out = cached;
-    return cudaSuccess;
-  }
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, uint32_t> cached;
   int dev = 0, sms = 0, per_sm = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return e;
+  const auto key = std::make_pair(reinterpret_cast<const void*>(kernel), dev);
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = cached.find(key);
+    if (it != cached.end()) {
+      out = it->second;
+      return cudaSuccess;
+    }
+  }
   if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
   if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, FAST_BLOCK, 0)) != cudaSuccess) return e;
-  cached = out = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+  out = (uint32_t)sms * (uint32_t)(per_sm > 0 ? per_sm : 1);
+  std::lock_guard<std::mutex> lock(mu);
+  cached[key] = out;
   return cudaSuccess;
 }
 

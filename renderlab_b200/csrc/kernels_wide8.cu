@@ -51,6 +51,24 @@ cudaError_t run(K kernel, const uint32_t* words, const rtk::W8View& v, const Src
   return cudaGetLastError();
 }
 
+// The f64 final pass of a closest-hit launch (rtk::k_wide8_final), on the walk's stream.
+template <class Src>
+cudaError_t final_pass(const SceneView& s, const rtk::W8View& v, const Src& src, uint32_t n, cudaStream_t stream) {
+  if (n == 0) return cudaSuccess;
+  const uint32_t blocks = (n + 255) / 256;
+  if (s.layout == 0) rtk::k_wide8_final<0><<<blocks, 256, 0, stream>>>(s.words, v, src, n);
+  else rtk::k_wide8_final<1><<<blocks, 256, 0, stream>>>(s.words, v, src, n);
+  return cudaGetLastError();
+}
+
+// A launch's walk followed, where it answers closest-hit queries, by the final pass.
+template <class Src>
+cudaError_t then_final(cudaError_t walk, bool closest, const SceneView& s, const rtk::W8View& v, const Src& src,
+                       uint32_t n, cudaStream_t stream) {
+  if (walk != cudaSuccess || !closest) return walk;
+  return final_pass(s, v, src, n, stream);
+}
+
 bool view_of(const SceneView& s, rtk::W8View& v) {
   if (!s.wide8) return false;
   const uint32_t* base = static_cast<const uint32_t*>(s.wide8);
@@ -69,12 +87,15 @@ cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, co
   if (!view_of(s, v)) return cudaErrorInvalidValue;
   using rtk::OneBatch;
   const OneBatch src{rays, order, hits};
+  cudaError_t e;
   if (s.layout == 0) {
-    if (mode == 0) return run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
-    return run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
+    e = mode == 0 ? run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill)
+                  : run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
+  } else {
+    e = mode == 0 ? run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill)
+                  : run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
   }
-  if (mode == 0) return run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
-  return run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
+  return then_final(e, mode == 0, s, v, src, n, stream);
 }
 
 bool shared_stack_fits(const SceneView& s) { return s.w8_depth <= rtk::W8_SSTACK; }
@@ -102,15 +123,19 @@ cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* tabl
   const ManyBatches src{table, entries, order};
 #define RT_W8B(L, AM, SS) \
   run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches, SS>, s.words, v, src, counter, total, st, stream, nullptr, refill)
+  cudaError_t e;
   if (stack == 0) {
-    if (s.layout == 0) return uniform_mode == 0 ? RT_W8B(0, 0, 0) : (uniform_mode == 1 ? RT_W8B(0, 1, 0) : RT_W8B(0, 2, 0));
-    return uniform_mode == 0 ? RT_W8B(1, 0, 0) : (uniform_mode == 1 ? RT_W8B(1, 1, 0) : RT_W8B(1, 2, 0));
+    if (s.layout == 0) e = uniform_mode == 0 ? RT_W8B(0, 0, 0) : (uniform_mode == 1 ? RT_W8B(0, 1, 0) : RT_W8B(0, 2, 0));
+    else e = uniform_mode == 0 ? RT_W8B(1, 0, 0) : (uniform_mode == 1 ? RT_W8B(1, 1, 0) : RT_W8B(1, 2, 0));
+  } else {
+    if (!shared_stack_fits(s)) return cudaErrorInvalidValue;
+    constexpr int SS = (int)rtk::W8_SSTACK;
+    if (s.layout == 0) e = uniform_mode == 0 ? RT_W8B(0, 0, SS) : (uniform_mode == 1 ? RT_W8B(0, 1, SS) : RT_W8B(0, 2, SS));
+    else e = uniform_mode == 0 ? RT_W8B(1, 0, SS) : (uniform_mode == 1 ? RT_W8B(1, 1, SS) : RT_W8B(1, 2, SS));
   }
-  if (!shared_stack_fits(s)) return cudaErrorInvalidValue;
-  constexpr int SS = (int)rtk::W8_SSTACK;
-  if (s.layout == 0) return uniform_mode == 0 ? RT_W8B(0, 0, SS) : (uniform_mode == 1 ? RT_W8B(0, 1, SS) : RT_W8B(0, 2, SS));
-  return uniform_mode == 0 ? RT_W8B(1, 0, SS) : (uniform_mode == 1 ? RT_W8B(1, 1, SS) : RT_W8B(1, 2, SS));
 #undef RT_W8B
+  // an all any-hit launch has no closest hits to finish; a mixed one skips its any-hit entries
+  return then_final(e, uniform_mode != 1, s, v, src, total, stream);
 }
 
 namespace {
@@ -134,12 +159,15 @@ cudaError_t launch_wide8_packet(const SceneView& s, uint32_t mode, const float4*
   if (!view_of(s, v) || s.top != 0) return cudaErrorInvalidValue;
   using rtk::OneBatch;
   const OneBatch src{rays, order, hits};
+  cudaError_t e;
   if (s.layout == 0) {
-    if (mode == 0) return run_packet(rtk::k_wide8_packet<0, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
-    return run_packet(rtk::k_wide8_packet<0, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+    e = mode == 0 ? run_packet(rtk::k_wide8_packet<0, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream)
+                  : run_packet(rtk::k_wide8_packet<0, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+  } else {
+    e = mode == 0 ? run_packet(rtk::k_wide8_packet<1, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream)
+                  : run_packet(rtk::k_wide8_packet<1, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
   }
-  if (mode == 0) return run_packet(rtk::k_wide8_packet<1, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
-  return run_packet(rtk::k_wide8_packet<1, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
+  return then_final(e, mode == 0, s, v, src, n, stream);
 }
 
 cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries,
@@ -151,9 +179,11 @@ cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntr
   using rtk::ManyBatches;
   const ManyBatches src{table, entries, order};
 #define RT_W8P(L, AM) run_packet(rtk::k_wide8_packet<L, AM, W8_BLOCK, ManyBatches>, s.words, v, src, counter, total, st, stream)
-  if (s.layout == 0) return uniform_mode == 0 ? RT_W8P(0, 0) : (uniform_mode == 1 ? RT_W8P(0, 1) : RT_W8P(0, 2));
-  return uniform_mode == 0 ? RT_W8P(1, 0) : (uniform_mode == 1 ? RT_W8P(1, 1) : RT_W8P(1, 2));
+  cudaError_t e;
+  if (s.layout == 0) e = uniform_mode == 0 ? RT_W8P(0, 0) : (uniform_mode == 1 ? RT_W8P(0, 1) : RT_W8P(0, 2));
+  else e = uniform_mode == 0 ? RT_W8P(1, 0) : (uniform_mode == 1 ? RT_W8P(1, 1) : RT_W8P(1, 2));
 #undef RT_W8P
+  return then_final(e, uniform_mode != 1, s, v, src, total, stream);
 }
 
 }  // namespace rtl

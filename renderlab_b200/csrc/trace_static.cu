@@ -13,6 +13,10 @@
 // current, through cudaGetSymbolAddress, and passes that pointer to the kernel. Every call
 // zeroes the counter and status on its stream before the launch and then shares the array with
 // every other call, so calls that overlap on the GPU race on it.
+//
+// Stack overflows: a push onto a full traversal stack is dropped and counted in the array's
+// status words, as a context counts it. rt_trace_static_stack_drops reads that count back after
+// the call's stream has finished; the next call on the device zeroes it.
 #include <cuda_runtime.h>
 
 #include <mutex>
@@ -52,7 +56,9 @@ extern "C" rt_status rt_trace_static(rt_layout layout, const uint32_t* d_words, 
   if (n > RT_STATIC_MAX_RAYS) return RT_ERR_INVALID_ARG;  // the ray counter's headroom
   if (n == 0) return RT_OK;
   if (!d_words || !d_rays || !d_hits || n_words < (layout == RT_LAYOUT_GI ? 16u : 8u)) return RT_ERR_INVALID_ARG;
-  if (reinterpret_cast<uintptr_t>(d_rays) % 16 != 0 || reinterpret_cast<uintptr_t>(d_words) % 16 != 0)
+  // rays and words are read in 16-byte loads, hits written as 4-byte words (as rt_trace_ex checks)
+  if (reinterpret_cast<uintptr_t>(d_rays) % 16 != 0 || reinterpret_cast<uintptr_t>(d_words) % 16 != 0 ||
+      reinterpret_cast<uintptr_t>(d_hits) % 4 != 0)
     return RT_ERR_INVALID_ARG;
   int device = 0;
   if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= MAX_DEVICES) return RT_ERR_CUDA;
@@ -67,4 +73,19 @@ extern "C" rt_status rt_trace_static(rt_layout layout, const uint32_t* d_words, 
   cudaError_t e = rtl::launch_fast(v, (uint32_t)mode, reinterpret_cast<const float4*>(d_rays), nullptr, d_hits, n,
                                    scratch, reinterpret_cast<rtk::DevStatus*>(scratch + 16), s, 8);
   return e == cudaSuccess ? RT_OK : RT_ERR_CUDA;
+}
+
+extern "C" rt_status rt_trace_static_stack_drops(void* stream, uint64_t* out) {
+  if (!out) return RT_ERR_INVALID_ARG;
+  int device = 0;
+  if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= MAX_DEVICES) return RT_ERR_CUDA;
+  unsigned int* scratch = nullptr;
+  if (scratch_for(device, &scratch) != cudaSuccess) return RT_ERR_CUDA;
+  cudaStream_t s = static_cast<cudaStream_t>(stream);
+  // the status words sit at word 16 of the array: DevStatus::stack_drops is their first member
+  unsigned long long drops = 0;
+  if (cudaMemcpyAsync(&drops, scratch + 16, sizeof drops, cudaMemcpyDeviceToHost, s) != cudaSuccess) return RT_ERR_CUDA;
+  if (cudaStreamSynchronize(s) != cudaSuccess) return RT_ERR_CUDA;
+  *out = drops;
+  return RT_OK;
 }

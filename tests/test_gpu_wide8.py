@@ -3,8 +3,10 @@ uncertain candidates) against the FP64 oracle (crates/asset/src/cluster_bvh/refe
 restated over the packed buffers).
 
 Tolerances: hit identity must equal the FP64 oracle's except on near ties, defined as both
-hitting with |t - t64| <= 1e-6 * t64; t within 1e-5 relative of t64 on every hit; any-hit
-flags equal except where the FP64 hit lies within 1e-5 relative of tmin or tmax."""
+hitting with |t - t64| <= 1e-6 * t64; t within 1e-5 relative of t64 on every hit; barycentrics
+u, v within 1e-5 of the oracle's on every hit with the oracle's identity (they range over [0, 1],
+so the bound is relative to that range); any-hit flags equal except where the FP64 hit lies
+within 1e-5 relative of tmin or tmax."""
 from __future__ import annotations
 
 import numpy as np
@@ -21,18 +23,22 @@ pytestmark = pytest.mark.gpu
 
 T_REL = 1e-5
 TIE_REL = 1e-6
+BARY_ABS = 1e-5
 
 
 def check_closest(layout, got, ref64, ident64, what):
-    """Returns (max rel t error, mean rel t error, near ties) and asserts the bar."""
+    """Returns (max rel t error, mean rel t error, near ties, max barycentric error) and asserts
+    the bar."""
     if layout == A.LAYOUT_GI:
         ghit = got[:, 1] != A.MISS
         gid = got[:, 1:5]
         oid = ident64[:, 2:6]
+        guv = got[:, 5:7]
     else:
         ghit = got[:, 1] != 0
         gid = got[:, 1:3]
         oid = ident64[:, 2:4]
+        guv = got[:, 3:5]
     ohit = ref64[:, 0] > 0
     t = got[:, 0].view(np.float32).astype(np.float64)
     t64 = ref64[:, 1]
@@ -46,7 +52,14 @@ def check_closest(layout, got, ref64, ident64, what):
                            f"got {got[bad[:2]]} oracle hit {ohit[bad[:2]]} t64 {t64[bad[:2]]} ident {oid[bad[:2]]}")
     if both.any():
         assert rel.max() <= T_REL, f"{what}: max rel t error {rel.max():.3g}"
-    return (float(rel.max()) if both.any() else 0.0, float(rel.mean()) if both.any() else 0.0, int(tie.sum()))
+    same = both & same_id
+    bary = np.abs(guv[same].view(np.float32).astype(np.float64) - ref64[same, 2:4]).max(axis=1) if same.any() else np.zeros(0)
+    if len(bary):
+        worst = np.nonzero(same)[0][np.argmax(bary)]
+        assert bary.max() <= BARY_ABS, (f"{what}: max barycentric error {bary.max():.3g} at ray {worst}: "
+                                        f"got {guv[worst].view(np.float32)} oracle {ref64[worst, 2:4]}")
+    return (float(rel.max()) if both.any() else 0.0, float(rel.mean()) if both.any() else 0.0, int(tie.sum()),
+            float(bary.max()) if len(bary) else 0.0)
 
 
 def check_any(got, rays, ref64, what):
