@@ -223,6 +223,26 @@ rt_status rt_gi_cell_rays(rt_ctx* ctx, const rt_gi_cell* d_cells, uint32_t n_cel
  * keeps the negation as a bit). Results at d_hits[c * 64 + k]. */
 rt_status rt_trace_gi_cells(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, const rt_gi_cell* d_cells,
                             uint32_t n_cells, uint32_t flags, void* d_hits, void* stream);
+/* The GI cache's per-light visibility (gi_light, shaders/gi_cache.wgsl:2040-2077): for every cell
+ * and light, whether the light reaches the cell (gi_light_affects, :2028-2036: lit, in front of
+ * the cell's surface, within range, inside a spot cone) and, if so, whether gi_visible_within
+ * finds nothing on the ray from the cell's offset origin (the gather rays' origin) toward it
+ * (gi_light_direction, :1977-1983; tmax the light's distance, 1e20 for a directional light).
+ * The rays are made inside the traversal's ray refill (no ray buffer). d_words receives
+ * ceil(n_lights / 32) words a cell: bit l % 32 of word l / 32 set when light l reaches the cell
+ * and its ray is clear. kernel: RT_KERNEL_FAST (bit-exact with the reference arithmetic) or
+ * RT_KERNEL_WIDE8 (after rt_scene_prepare). The cache state around gi_light -- its shade queue,
+ * the light-reuse and moved-caster shortcuts -- is the renderer's and not part of this call. */
+typedef struct rt_gi_light { /* light_cluster.wgsl:10, 80 bytes */
+  float position_range[4];
+  float travel_outer[4];
+  float rgb_inner[4];
+  uint32_t kind[4]; /* kind[0]: 0 directional, 1 point, 2 spot */
+  float source[4];
+} rt_gi_light;
+rt_status rt_trace_gi_lights(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const rt_gi_cell* d_cells,
+                             uint32_t n_cells, const rt_gi_light* d_lights, uint32_t n_lights, uint32_t* d_words,
+                             void* stream);
 
 /* ---- Many batches in one launch ----------------------------------------------------------
  * Uneven ray batches of one scene, each with its own buffers and mode, traced by ONE persistent
@@ -300,6 +320,12 @@ rt_status rt_server_submit(rt_server* srv, uint32_t scene, rt_mode mode, const r
  * Returns the request's status and forgets the ticket. */
 rt_status rt_server_wait(rt_server* srv, uint64_t ticket, int32_t timeout_ms);
 rt_status rt_server_get_stats(rt_server* srv, rt_server_stats* out, int reset);
+/* Failure injection on the host, for tests of the serving loop's error path: the next `launches`
+ * slot launches fail with `status` (not RT_OK) before anything of them is enqueued, as a failing
+ * copy or launch call would (the reference's Error::Fault, src/lib.rs:138-160). Every request
+ * with rays in such a slot finishes with that status; the slot returns to service and later
+ * requests run normally. 0 launches clears it. No device fault is involved. */
+rt_status rt_server_fail_next(rt_server* srv, uint32_t launches, rt_status status);
 /* Finishes every submitted request, then frees the slots and releases the scenes. */
 rt_status rt_server_destroy(rt_server* srv);
 

@@ -102,8 +102,8 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_trace_host_batches", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
-           "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
-           "rt_server_wait", "rt_server_get_stats", "rt_server_destroy",
+           "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_trace_gi_lights", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
+           "rt_server_wait", "rt_server_get_stats", "rt_server_fail_next", "rt_server_destroy",
            "rt_trace_static", "rt_trace_static_stack_drops", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
            "rt_scene_move_instances", "rt_blas_build", "rt_blas_build_device", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_build_device", "rt_tlas_refit", "rt_blas_positions",
@@ -161,6 +161,7 @@ def lib() -> ctypes.CDLL:
     L.rt_scene_refit.argtypes = [_vp, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp]
     L.rt_gi_cell_rays.argtypes = [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]
     L.rt_trace_gi_cells.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, _vp]
+    L.rt_trace_gi_lights.argtypes = [_vp, _vp, ctypes.c_int, _vp, ctypes.c_uint32, _vp, ctypes.c_uint32, _vp, _vp]
     L.rt_scene_read_words.argtypes = [_vp, _vp, ctypes.c_size_t, ctypes.c_size_t, _u32p]
     L.rt_server_create.argtypes = [_vp, ctypes.POINTER(RtServerDesc), ctypes.POINTER(_vp)]
     L.rt_server_add_scene.argtypes = [_vp, ctypes.c_int, _u32p, ctypes.c_size_t, _u32p]
@@ -169,6 +170,7 @@ def lib() -> ctypes.CDLL:
                                    ctypes.POINTER(ctypes.c_uint64)]
     L.rt_server_wait.argtypes = [_vp, ctypes.c_uint64, ctypes.c_int32]
     L.rt_server_get_stats.argtypes = [_vp, ctypes.POINTER(RtServerStats), ctypes.c_int]
+    L.rt_server_fail_next.argtypes = [_vp, ctypes.c_uint32, ctypes.c_int]
     L.rt_server_destroy.argtypes = [_vp]
     L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_static_stack_drops.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64)]
@@ -555,9 +557,14 @@ class Server:
         st = lib().rt_server_wait(self.handle, ticket, timeout_ms)
         if st == 5:
             raise RtError(st, "request still running")
-        rays, out = self._held.pop(ticket)
+        rays, out = self._held.pop(ticket, (None, None))  # released once waited for, whatever the status
         self.engine._check(st)
         return out
+
+    def fail_next(self, launches: int, status: int = 6):
+        """rt_server_fail_next: the next `launches` slot launches fail on the host with `status`
+        (default RT_ERR_CUDA) before anything is enqueued -- failure injection for tests."""
+        self.engine._check(lib().rt_server_fail_next(self.handle, launches, status))
 
     def stats(self, reset: bool = False) -> dict:
         s = RtServerStats()
@@ -733,6 +740,23 @@ class Engine:
         self._check(lib().rt_trace_gi_cells(self.ctx, scene.handle, mode, cells.data_ptr(), cells.shape[0],
                                             GI_ROTATE if rotate else 0, hits.data_ptr(), s))
         return hits
+
+    def trace_gi_lights(self, scene: Scene, cells, lights, kernel: str = "fast", out=None, stream=None):
+        """gi_light's visibility words (GI layout): cells (n, 8) and lights (m, 20) 32-bit CUDA
+        tensors (rt_gi_cell / rt_gi_light records); returns (n, ceil(m / 32)) int32 words, bit
+        l % 32 of word l / 32 set when light l reaches the cell and nothing blocks its ray."""
+        import torch
+        n, m = cells.shape[0], lights.shape[0]
+        if cells.shape[1:] != (8,) or lights.shape[1:] != (20,) or cells.element_size() != 4 or lights.element_size() != 4:
+            raise ValueError("cells must be (n, 8) and lights (m, 20) tensors of 32-bit words")
+        if not cells.is_contiguous() or not lights.is_contiguous():
+            raise ValueError("cells and lights must be contiguous")
+        if out is None:
+            out = torch.empty((n, (m + 31) // 32), dtype=torch.int32, device=cells.device)
+        s = stream if stream is not None else torch.cuda.current_stream().cuda_stream
+        self._check(lib().rt_trace_gi_lights(self.ctx, scene.handle, KERNELS[kernel], cells.data_ptr(), n,
+                                             lights.data_ptr(), m, out.data_ptr(), s))
+        return out
 
     def order(self, scene: Scene, rays, key: str = "octant", out=None, stream=None):
         """A permutation of `rays` (CUDA tensor) grouping alike rays; int32 CUDA tensor."""

@@ -92,4 +92,80 @@ RT_DEV Ray fetch(const CellRays& s, uint32_t id, Lane& L) {
 }
 RT_DEV void* out_of(const CellRays& s, uint32_t) { return s.out; }
 
+// ---- per-light visibility (gi_light, gi_cache.wgsl:2040-2077) ----
+
+// A light as the GI cache reads it (light_cluster.wgsl:10, 80 bytes): position and range,
+// travel direction and spot cosine, colour and inner cosine, kind (x: 0 directional, 1 point,
+// 2 spot), source.
+struct GiLight {
+  float position_range[4];
+  float travel_outer[4];
+  float rgb_inner[4];
+  uint32_t kind[4];
+  float source[4];
+};
+
+// gi_light_direction (gi_cache.wgsl:1977-1983): the unit direction from q toward the light and
+// its distance (1e20 for a directional light).
+RT_DEV void gi_light_direction(const GiLight& l, F3 q, F3& d, float& dist) {
+  if (l.kind[0] == 0u) {
+    d = {-l.travel_outer[0], -l.travel_outer[1], -l.travel_outer[2]};
+    dist = 1e20f;
+    return;
+  }
+  const F3 e = {sub(l.position_range[0], q.x), sub(l.position_range[1], q.y), sub(l.position_range[2], q.z)};
+  dist = __fsqrt_rn(dot3(e, e));
+  const float den = fmaxf(dist, 1e-30f);
+  d = {__fdiv_rn(e.x, den), __fdiv_rn(e.y, den), __fdiv_rn(e.z, den)};
+}
+
+// gi_light_affects (gi_cache.wgsl:2028-2036): a lit light whose direction leaves the cell's
+// surface, within range, and inside a spot light's cone.
+RT_DEV bool gi_light_affects(const GiLight& l, F3 n, F3 d, float dist) {
+  if (l.rgb_inner[0] == 0.0f && l.rgb_inner[1] == 0.0f && l.rgb_inner[2] == 0.0f) return false;
+  if (dot3(n, d) <= 0.0f) return false;
+  if (l.kind[0] == 0u) return true;
+  if (l.position_range[3] > 0.0f && dist >= l.position_range[3]) return false;
+  return l.kind[0] != 2u || dot3({-d.x, -d.y, -d.z}, {l.travel_outer[0], l.travel_outer[1], l.travel_outer[2]}) > l.travel_outer[3];
+}
+
+// Ray source: item i is (cell i / n_lights, light i % n_lights), the ray gi_light traces with
+// gi_visible_within from the cell's offset origin toward the light (tmin 0, tmax the light's
+// distance from the query point). A light that does not reach the cell is not traced: its ray
+// gets tmax -1, which nothing meets, and no bit. Results are the cells' light words: bit l % 32
+// of word l / 32 of cell c (words_per_cell words a cell, zeroed before the launch) is set when
+// the light reaches the cell and nothing blocks its ray.
+struct LightRays {
+  const GiCell* cells;
+  const GiLight* lights;
+  uint32_t n_lights;
+  uint32_t words_per_cell;
+  uint32_t* words;
+};
+RT_DEV Ray gi_light_ray(const LightRays& s, uint32_t i) {
+  const uint32_t c = i / s.n_lights, l = i - c * s.n_lights;
+  const GiCell& cell = s.cells[c];
+  const F3 q = {cell.q[0], cell.q[1], cell.q[2]};
+  const F3 n = gi_unpack_normal(cell.normal);
+  const float off = gi_origin_offset(q, cell.edge);
+  const F3 o = {add(q.x, mul(n.x, off)), add(q.y, mul(n.y, off)), add(q.z, mul(n.z, off))};
+  const GiLight& light = s.lights[l];
+  F3 d;
+  float dist;
+  gi_light_direction(light, q, d, dist);
+  return Ray{o, 0.0f, d, gi_light_affects(light, n, d, dist) ? dist : -1.0f};
+}
+template <class Lane>
+RT_DEV Ray fetch(const LightRays& s, uint32_t id, Lane& L) {
+  L.ray_id = id;
+  L.entry = 0;
+  return gi_light_ray(s, id);
+}
+RT_DEV void* out_of(const LightRays& s, uint32_t) { return s.words; }
+RT_DEV void put_flag(const LightRays& s, uint32_t, uint32_t id, const Ray& ray, bool blocked) {
+  if (blocked || !(ray.tmax > 0.0f)) return;
+  const uint32_t c = id / s.n_lights, l = id - c * s.n_lights;
+  atomicOr(s.words + (size_t)c * s.words_per_cell + (l >> 5), 1u << (l & 31u));
+}
+
 }  // namespace rtk

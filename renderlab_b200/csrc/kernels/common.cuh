@@ -133,6 +133,13 @@ RT_DEV Ray fetch(const ManyBatches& s, uint32_t id, Lane& L) {
 RT_DEV void* out_of(const OneBatch& s, uint32_t) { return s.out; }
 RT_DEV void* out_of(const ManyBatches& s, uint32_t entry) { return s.table[entry].hits; }
 
+// Stores an any-hit result: one word a ray, 1 when something blocks it. A ray source that packs
+// its results otherwise (the GI cache's light words) overloads this for its own type.
+template <class Src>
+RT_DEV void put_flag(const Src& s, uint32_t entry, uint32_t id, const Ray&, bool blocked) {
+  reinterpret_cast<uint32_t*>(out_of(s, entry))[id] = blocked ? 1u : 0u;
+}
+
 // Device-side counters every traversal kernel may bump (rare events only).
 struct DevStatus {
   unsigned long long stack_drops;

@@ -67,12 +67,12 @@ struct RsLane {
   uint32_t sp;
 };
 
-template <int AM>
-RT_DEV void rs_finish(RsLane<AM>& L, void* __restrict__ out) {
+template <int AM, class Src>
+RT_DEV void rs_finish(RsLane<AM>& L, const Src& src) {
   if (any_of<AM>(L)) {
-    reinterpret_cast<uint32_t*>(out)[L.ray_id] = L.best.rec[0] != 0 ? 1u : 0u;
+    put_flag(src, L.entry, L.ray_id, L.ray, L.best.rec[0] != 0);
   } else {
-    uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * (size_t)L.ray_id;
+    uint32_t* o = reinterpret_cast<uint32_t*>(out_of(src, L.entry)) + 5 * (size_t)L.ray_id;
     o[0] = __float_as_uint(L.best.t), o[1] = L.best.rec[0], o[2] = L.best.rec[1], o[3] = L.best.rec[2];
     o[4] = L.best.rec[3];
   }
@@ -219,7 +219,7 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
         L.tsp = 1;
         top_stack[0] = head.z;
       } else {
-        rs_finish<AM>(L, out_of(src, L.entry));  // misses the scene box: done, refilled next iteration
+        rs_finish<AM>(L, src);  // misses the scene box: done, refilled next iteration
       }
     }
     // Every lane reaches this vote once per iteration (no exit above it); the warp leaves only
@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
         const uint32_t child = L.cur;
         if (child & LEAF) {
           if (rs_leaf<AM>(w, L, child)) {
-            rs_finish<AM>(L, out_of(src, L.entry));
+            rs_finish<AM>(L, src);
             continue;
           }
           L.cur = EMPTY;
@@ -253,14 +253,14 @@ __global__ void __launch_bounds__(BLOCK) k_rs_fast(const uint32_t* __restrict__ 
     if (L.phase == PH_TOP) {
       if (head.y == 0) {  // flat instance list
         if (L.flat_i >= head.x) {
-          rs_finish<AM>(L, out_of(src, L.entry));
+          rs_finish<AM>(L, src);
           continue;
         }
         rs_enter<AM>(w, L, L.flat_i++);
         continue;
       }
       if (L.tsp == 0) {
-        rs_finish<AM>(L, out_of(src, L.entry));
+        rs_finish<AM>(L, src);
         continue;
       }
       const uint32_t item = top_stack[--L.tsp];
@@ -293,13 +293,13 @@ struct GiLane {
   uint32_t cur, sp;
 };
 
-template <int AM>
-RT_DEV void gi_finish(GiLane<AM>& L, void* __restrict__ out) {
+template <int AM, class Src>
+RT_DEV void gi_finish(GiLane<AM>& L, const Src& src) {
   const GiBest& b = L.best;
   if (any_of<AM>(L)) {
-    reinterpret_cast<uint32_t*>(out)[L.ray_id] = b.hit ? 1u : 0u;
+    put_flag(src, L.entry, L.ray_id, L.ray, b.hit);
   } else {
-    uint32_t* o = reinterpret_cast<uint32_t*>(out) + 10 * (size_t)L.ray_id;
+    uint32_t* o = reinterpret_cast<uint32_t*>(out_of(src, L.entry)) + 10 * (size_t)L.ray_id;
     o[0] = __float_as_uint(b.t), o[1] = b.inst, o[2] = b.tri[0], o[3] = b.tri[1], o[4] = b.tri[2];
     o[5] = __float_as_uint(b.u), o[6] = __float_as_uint(b.v);
     o[7] = __float_as_uint(b.n.x), o[8] = __float_as_uint(b.n.y), o[9] = __float_as_uint(b.n.z);
@@ -443,7 +443,7 @@ __global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ 
         const uint32_t child = L.cur;
         if (child & LEAF) {
           if (gi_leaf<AM>(w, L, child)) {
-            gi_finish<AM>(L, out_of(src, L.entry));
+            gi_finish<AM>(L, src);
             continue;
           }
           L.cur = EMPTY;
@@ -456,14 +456,14 @@ __global__ void __launch_bounds__(BLOCK) k_gi_fast(const uint32_t* __restrict__ 
     if (L.phase == PH_TOP) {
       if (top == 0) {
         if (L.flat_i >= instances) {
-          gi_finish<AM>(L, out_of(src, L.entry));
+          gi_finish<AM>(L, src);
           continue;
         }
         gi_enter<AM>(w, L, L.flat_i++);
         continue;
       }
       if (L.tsp == 0) {
-        gi_finish<AM>(L, out_of(src, L.entry));
+        gi_finish<AM>(L, src);
         continue;
       }
       const uint32_t item = top_stack[--L.tsp];

@@ -454,17 +454,18 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
 // estimate, the record's identity words and, in the words k_wide8_final overwrites, the instance
 // and 8-wide triangle that pass needs (reflection: u <- instance, v <- triangle; GI: word 2 <-
 // triangle). A miss is written in full here.
-template <uint32_t LAYOUT, int AM, bool COUNT>
-RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, void* __restrict__ out,
+template <uint32_t LAYOUT, int AM, bool COUNT, class Src>
+RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, const Src& src,
                       unsigned long long* cnt) {
   w8_count<COUNT>(cnt, W8C_RAYS);
   W8Best& b = L.best;
   const uint32_t id = L.ray_id;
   L.phase = 0;
   if (any_of<AM>(L)) {
-    reinterpret_cast<uint32_t*>(out)[id] = b.hit ? 1u : 0u;
+    put_flag(src, L.entry, id, L.ray, b.hit);
     return;
   }
+  void* __restrict__ out = out_of(src, L.entry);
   if (b.hit) w8_count<COUNT>(cnt, W8C_FINAL64);
   if (LAYOUT == 1) {
     uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * (size_t)id;
@@ -630,21 +631,21 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       if (L.node == EMPTY && !w8_next(L, stack)) {
         L.phase = 1;
       } else {
-        if (w8_node<LAYOUT, AM, COUNT>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, AM, COUNT>(w, V, L, out_of(src, L.entry), cnt);
+        if (w8_node<LAYOUT, AM, COUNT>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
         continue;
       }
     }
     if (L.phase == 1) {
       if (top == 0) {
         if (L.flat >= count) {
-          w8_finish<LAYOUT, AM, COUNT>(w, V, L, out_of(src, L.entry), cnt);
+          w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
           continue;
         }
         w8_enter<LAYOUT, AM, COUNT>(w, V, L, L.flat++, cnt);
         continue;
       }
       if (L.tsp == 0) {
-        w8_finish<LAYOUT, AM, COUNT>(w, V, L, out_of(src, L.entry), cnt);
+        w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
         continue;
       }
       const uint32_t item = tstack[--L.tsp];
@@ -748,7 +749,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8_packet(const 
         }
       }
     }
-    if (id < n) w8_finish<LAYOUT, AM, false>(w, V, L, out_of(src, L.entry), nullptr);
+    if (id < n) w8_finish<LAYOUT, AM, false>(w, V, L, src, nullptr);
   }
 }
 

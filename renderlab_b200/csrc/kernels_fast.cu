@@ -102,4 +102,18 @@ cudaError_t launch_fast_cells(const SceneView& s, uint32_t mode, const void* cel
   return run(rtk::k_gi_fast<1, FAST_BLOCK, CellRays>, s, src, items, counter, st, stream, refill);
 }
 
+cudaError_t launch_fast_lights(const SceneView& s, const void* cells, uint32_t n_cells, const void* lights,
+                               uint32_t n_lights, uint32_t* words, unsigned int* counter, rtk::DevStatus* st,
+                               cudaStream_t stream, uint32_t refill) {
+  if (s.layout != 0) return cudaErrorInvalidValue;
+  const uint32_t per_cell = (n_lights + 31) / 32, items = n_cells * n_lights;
+  if (n_cells == 0 || n_lights == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(words, 0, (size_t)n_cells * per_cell * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  using rtk::LightRays;
+  const LightRays src{static_cast<const rtk::GiCell*>(cells), static_cast<const rtk::GiLight*>(lights), n_lights, per_cell,
+                      words};
+  return run(rtk::k_gi_fast<1, FAST_BLOCK, LightRays>, s, src, items, counter, st, stream, refill);
+}
+
 }  // namespace rtl

@@ -2,6 +2,7 @@
 #include <map>
 #include <mutex>
 
+#include "kernels/cells.cuh"
 #include "kernels/wide8.cuh"
 #include "launch.hpp"
 
@@ -136,6 +137,24 @@ cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* tabl
 #undef RT_W8B
   // an all any-hit launch has no closest hits to finish; a mixed one skips its any-hit entries
   return then_final(e, uniform_mode != 1, s, v, src, total, stream);
+}
+
+cudaError_t launch_wide8_lights(const SceneView& s, const void* cells, uint32_t n_cells, const void* lights,
+                                uint32_t n_lights, uint32_t* words, unsigned int* counter, rtk::DevStatus* st,
+                                cudaStream_t stream, uint32_t refill, uint32_t stack) {
+  rtk::W8View v;
+  if (s.layout != 0 || !view_of(s, v)) return cudaErrorInvalidValue;
+  const uint32_t per_cell = (n_lights + 31) / 32, items = n_cells * n_lights;
+  if (n_cells == 0 || n_lights == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(words, 0, (size_t)n_cells * per_cell * sizeof(uint32_t), stream);
+  if (e != cudaSuccess) return e;
+  using rtk::LightRays;
+  const LightRays src{static_cast<const rtk::GiCell*>(cells), static_cast<const rtk::GiLight*>(lights), n_lights, per_cell,
+                      words};
+  if (stack == 0) return run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, 0>, s.words, v, src, counter, items, st, stream, nullptr, refill);
+  if (!shared_stack_fits(s)) return cudaErrorInvalidValue;
+  return run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, (int)rtk::W8_SSTACK>, s.words, v, src, counter, items, st, stream,
+             nullptr, refill);
 }
 
 namespace {

@@ -63,6 +63,15 @@ cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntr
 cudaError_t launch_cell_rays(const void* cells, uint32_t n_cells, uint32_t rotate, float4* rays, cudaStream_t stream);
 cudaError_t launch_fast_cells(const SceneView& s, uint32_t mode, const void* cells, uint32_t n_cells, uint32_t rotate,
                               void* hits, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, uint32_t refill);
+// The GI cache's per-light visibility (gi_light): item c * n_lights + l is cell c's ray toward
+// light l, traced any-hit (FAST or WIDE8, generated in the ray refill), results packed into
+// ceil(n_lights / 32) words a cell at `words` (zeroed on `stream` first).
+cudaError_t launch_fast_lights(const SceneView& s, const void* cells, uint32_t n_cells, const void* lights,
+                               uint32_t n_lights, uint32_t* words, unsigned int* counter, rtk::DevStatus* st,
+                               cudaStream_t stream, uint32_t refill);
+cudaError_t launch_wide8_lights(const SceneView& s, const void* cells, uint32_t n_cells, const void* lights,
+                                uint32_t n_lights, uint32_t* words, unsigned int* counter, rtk::DevStatus* st,
+                                cudaStream_t stream, uint32_t refill, uint32_t stack);
 // Ray ordering (kernels_order.cu): scratch holds the keys, the unsorted indices and the radix
 // sort's temporary storage.
 size_t order_scratch_bytes(uint32_t n);

@@ -628,6 +628,42 @@ rt_status rt_trace_gi_cells(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, co
   return RT_OK;
 }
 
+rt_status rt_trace_gi_lights(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const rt_gi_cell* d_cells,
+                             uint32_t n_cells, const rt_gi_light* d_lights, uint32_t n_lights, uint32_t* d_words,
+                             void* stream) {
+  rt_status s = check_trace_args(ctx, scene, RT_ANY_CASTERS, kernel);
+  if (s != RT_OK) return s;
+  if (scene->layout != RT_LAYOUT_GI) return fail(ctx, RT_ERR_INVALID_ARG, "the light producer traces GI-layout scenes");
+  if (kernel != RT_KERNEL_FAST && kernel != RT_KERNEL_WIDE8)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "light visibility is traced by RT_KERNEL_FAST or RT_KERNEL_WIDE8");
+  if (kernel == RT_KERNEL_WIDE8 && !scene->d_wide8)
+    return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare first");
+  if (n_cells == 0 || n_lights == 0) return RT_OK;
+  if (!d_cells || !d_lights || !d_words) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if ((uint64_t)n_cells * n_lights > (1ull << 31))
+    return fail(ctx, RT_ERR_INVALID_ARG, "at most 2^31 (cell, light) pairs a call");
+  if (reinterpret_cast<uintptr_t>(d_cells) % 16 != 0 || reinterpret_cast<uintptr_t>(d_lights) % 16 != 0 ||
+      reinterpret_cast<uintptr_t>(d_words) % 4 != 0)
+    return fail(ctx, RT_ERR_INVALID_ARG, "cells and lights must be 16-byte aligned, words 4-byte aligned");
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  const rtl::SceneView v = view_of(scene);
+  unsigned int* counter = ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS);
+  const cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaError_t e;
+  if (kernel == RT_KERNEL_FAST) {
+    e = rtl::launch_fast_lights(v, d_cells, n_cells, d_lights, n_lights, d_words, counter, ctx->d_status, st,
+                                ctx->tuning.fast_refill);
+  } else {
+    const uint32_t stack = ctx->tuning.wide8_stack == RT_STACK_SHARED && rtl::shared_stack_fits(v) ? 1u : 0u;
+    e = rtl::launch_wide8_lights(v, d_cells, n_cells, d_lights, n_lights, d_words, counter, ctx->d_status, st,
+                                 ctx->tuning.wide8_refill, stack);
+  }
+  if (e != cudaSuccess) return fail(ctx, RT_ERR_CUDA, "light visibility traversal: %s", cudaGetErrorString(e));
+  ctx->rays += (uint64_t)n_cells * n_lights;
+  ctx->launches += 1;
+  return RT_OK;
+}
+
 // ---------------------------------------------------------------- cooked files
 
 namespace {

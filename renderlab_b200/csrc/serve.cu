@@ -94,6 +94,9 @@ struct rt_server {
   std::thread worker;
   bool stop = false;
   uint64_t next_ticket = 1;
+  // rt_server_fail_next: slot launches still to fail on the host, and the status they fail with
+  uint32_t fail_launches = 0;
+  rt_status fail_status = RT_OK;
   // statistics since the last reset
   std::vector<double> latency_ms;
   uint64_t rays = 0, launches = 0, requests_done = 0;
@@ -194,8 +197,13 @@ void work(rt_server* srv) {
       fill(srv, s);
       uint32_t rays = 0;
       for (const Chunk& c : s.chunks) rays += c.n;
+      rt_status injected = RT_OK;
+      if (srv->fail_launches) {  // a fake of a failing enqueue: nothing of this slot is enqueued
+        srv->fail_launches -= 1;
+        injected = srv->fail_status;
+      }
       lock.unlock();  // copies from pageable memory block; new requests may arrive meanwhile
-      const rt_status st = launch(srv, s);
+      const rt_status st = injected != RT_OK ? injected : launch(srv, s);
       lock.lock();
       if (st != RT_OK) {  // nothing of this slot is in flight after a failed enqueue
         cudaStreamSynchronize(s.stream);
@@ -356,6 +364,14 @@ rt_status rt_server_wait(rt_server* srv, uint64_t ticket, int32_t timeout_ms) {
   srv->requests.erase(it);
   delete r;
   return st;
+}
+
+rt_status rt_server_fail_next(rt_server* srv, uint32_t launches, rt_status status) {
+  if (!srv || (launches && status == RT_OK)) return RT_ERR_INVALID_ARG;
+  std::lock_guard<std::mutex> lock(srv->mu);
+  srv->fail_launches = launches;
+  srv->fail_status = status;
+  return RT_OK;
 }
 
 rt_status rt_server_get_stats(rt_server* srv, rt_server_stats* out, int reset) {

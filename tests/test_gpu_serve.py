@@ -112,3 +112,58 @@ def test_admission_by_budget_and_busy_scene(engine):
         srv.remove_scene(sid)
     finally:
         srv.close()
+
+
+def test_a_bounded_wait_times_out_and_the_request_stays_waitable(engine):
+    """rt_server_wait with a limit returns RT_ERR_TIMEOUT while the request runs and keeps it:
+    a later wait returns its hits, equal to the rays traced alone."""
+    import torch
+    layout, words = _scenes()[2]
+    rays = H.random_rays(3_000_000, -60.0, 60.0, seed=11, tmax=300.0)
+    srv = A.Server(engine, hbm_budget=4 << 30, launch_rays=1 << 19, slots=2, kernel="fast")
+    try:
+        sid = srv.add_scene(layout, words)
+        t = srv.submit(sid, rays, A.CLOSEST)
+        with pytest.raises(A.RtError, match="TIMEOUT"):
+            srv.wait(t, timeout_ms=0)  # 3M rays through two 512k-ray slots: not done at once
+        got = srv.wait(t, timeout_ms=120_000)
+        sc = engine.upload(layout, words)
+        want = engine.trace(sc, torch.from_numpy(rays).cuda(), A.CLOSEST, "fast").cpu().numpy().view(np.uint32)
+        sc.release()
+        assert np.array_equal(got.reshape(want.shape), want)
+        with pytest.raises(A.RtError, match="INVALID_ARG"):  # a ticket is waited for once
+            srv.wait(t, timeout_ms=0)
+    finally:
+        srv.close()
+
+
+@pytest.mark.parametrize("kernel", ["fast", "wide8"])
+def test_a_failed_launch_fails_its_requests_and_the_server_carries_on(engine, kernel):
+    """A slot launch that fails on the host (injected: a fake of a failing copy or launch call,
+    no device fault) finishes every request with rays in that slot with the failure's status
+    instead of hanging them; the slot returns to service, later requests get correct hits, and
+    a submit for a scene that does not exist is refused at once."""
+    import torch
+    layout, words = _scenes()[1]
+    rays = H.random_rays(120_000, -60.0, 60.0, seed=12, tmax=300.0)
+    srv = A.Server(engine, hbm_budget=4 << 30, launch_rays=50_000, slots=1, kernel=kernel)
+    try:
+        sid = srv.add_scene(layout, words)
+        srv.fail_next(1, 6)  # RT_ERR_CUDA
+        t = srv.submit(sid, rays, A.CLOSEST)  # three slot launches: the first fails
+        with pytest.raises(A.RtError, match="CUDA"):
+            srv.wait(t, timeout_ms=120_000)
+        small = rays[:40_000]
+        t = srv.submit(sid, small, A.ANY_CASTERS)
+        got = srv.wait(t, timeout_ms=120_000)
+        sc = engine.upload(layout, words)
+        if kernel == "wide8":
+            sc.prepare("wide8")
+        want = engine.trace(sc, torch.from_numpy(small).cuda(), A.ANY_CASTERS, kernel).cpu().numpy().view(np.uint32)
+        sc.release()
+        assert np.array_equal(got.reshape(want.shape), want)
+        with pytest.raises(A.RtError, match="INVALID_ARG"):
+            srv.submit(sid + 7, small, A.CLOSEST)
+        assert srv.stats()["pending"] == 0
+    finally:
+        srv.close()
