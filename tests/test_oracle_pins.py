@@ -35,6 +35,43 @@ def test_replay_golden_vectors(case, any_hit):
     assert (hits[:, 1] != 0).sum() > 30
 
 
+GENERAL = H.__file__.replace("helpers.py", "golden/replay_bvh2_general.npz")
+
+
+@pytest.mark.parametrize("case", ["flat", "tlas"])
+@pytest.mark.parametrize("any_hit", [False, True])
+def test_replay_general_inputs(case, any_hit):
+    """tools/sunrt/replay_geometry.py over general f32 scenes (jittered height fields and
+    triangle soups, instances under arbitrary rotations and scales, 600 rays aimed at triangle
+    interiors, edges and vertices; tests/golden/make_replay_golden.py --general).
+
+    - "sequential": the replay with its np.dot summed left to right in f32 (the order the WGSL
+      writes and the oracle evaluates). The oracle must equal it bit for bit: t, hit records
+      with barycentric bits, and all nine traversal counters, on every ray.
+    - "numpy": the replay as it ships, np.dot from the host's BLAS (another summation order).
+      Rays aimed at triangle interiors or past them must give the same hit identity, with t
+      within 2e-5 relative; only rays aimed exactly at an edge or a vertex, where two triangles
+      are both hit within the reference's RS_EDGE slack, may resolve to the other one."""
+    g = np.load(GENERAL)
+    names = list(g["counters"])
+    idx = [O.COUNTERS.index(n) for n in names]
+    hits, cnt = O.rs_trace_counts(g[case + "_words"], g[case + "_rays"], any_hit=any_hit, bvh2=True)
+    key = f"{case}_{'any' if any_hit else 'closest'}"
+    seq = key + "_sequential"
+    assert np.array_equal(hits[:, 0], g[seq + "_t"])
+    assert np.array_equal(hits[:, 1:], g[seq + "_record"])
+    assert np.array_equal(cnt[:, idx], g[seq + "_counters"])
+    num = key + "_numpy"
+    rec, t = g[num + "_record"], g[num + "_t"].view(np.float32).astype(np.float64)
+    same = (hits[:, 1:3] == rec[:, 0:2]).all(1)
+    aim = np.arange(len(hits)) % 6  # 0, 1 interior; 2, 3 an edge; 4 a vertex; 5 past the triangle
+    assert same[(aim < 2) | (aim == 5)].all()
+    both = same & (rec[:, 0] != 0)
+    tt = hits[both, 0].view(np.float32).astype(np.float64)
+    assert np.all(np.abs(tt - t[both]) <= 2e-5 * np.abs(t[both]))
+    assert (rec[:, 0] != 0).sum() > 300 and same.mean() > 0.9
+
+
 def test_replay_known_answer_lower_instance_wins():
     """test_replay_geometry.py:43-85: two identity instances of one triangle; the equal-t hit
     resolves to the lower instance (slot 7 + 1) even when the top level visits instance 1 first."""
