@@ -34,9 +34,14 @@ constexpr uint32_t W8_STACK = 32;
 // Entries of the shared-memory group stack (a scene whose 8-wide trees are at most this many
 // levels deep stacks at most W8_SSTACK - 1 groups).
 constexpr uint32_t W8_SSTACK = 16;
-// Resident 128-thread blocks per SM the register allocation is sized for (4: 128 registers).
+// Resident 128-thread blocks per SM the register allocation is sized for: the per-ray walk
+// (RT_W8_MIN_BLOCKS) and the packet walk (RT_W8P_MIN_BLOCKS). The f64 paths and the lazy
+// instance setup are out of line, so the walks' hot loops fit these budgets.
 #ifndef RT_W8_MIN_BLOCKS
 #define RT_W8_MIN_BLOCKS 4
+#endif
+#ifndef RT_W8P_MIN_BLOCKS
+#define RT_W8P_MIN_BLOCKS 4
 #endif
 
 // Opt-in device counters of the WIDE8 walk (diagnostics and the bytes-per-ray roofline).
@@ -61,7 +66,6 @@ struct W8Best {
   uint32_t inst;    // instance index
   uint32_t tri;     // 8-wide triangle index
   uint32_t ident;   // primitive id (reflection) or triangle ordinal (GI)
-  float u, v;
 };
 
 // f64 reference arithmetic, never contracted (reference.rs:47-59).
@@ -127,7 +131,10 @@ __device__ __noinline__ bool mt64(const uint32_t* __restrict__ w, uint32_t inst,
   return t > (double)ray.tmin && t < (double)ray.tmax;
 }
 
-// Per-instance object-space ray state for the 8-wide walk.
+// Per-instance object-space ray state for the 8-wide walk. The walk's part (o, d, inv, oct) is
+// set when the instance is entered; the triangle test's part (the shear, oerr, tscale) when the
+// instance's first leaf triangle is tested (w8_shear): in scenes of many overlapping instances
+// most entered instances end at their root node's boxes, and never need it.
 struct W8Ray {
   F3 o, d, inv;
   uint32_t oct;
@@ -136,11 +143,21 @@ struct W8Ray {
   float oerr;   // |o - o64|_inf: the f32 object-space origin against the f64 reference's
   float tscale; // 8 u |1 / d_kz|: absolute error of t per unit of |v - o|
   bool valid;
+  bool sheared; // the triangle test's part is set
 };
 
+// The walk's part: reciprocal direction, octant, and whether the direction is usable at all.
 RT_DEV void w8_setup(W8Ray& R) {
   R.inv = safe_inverse(R.d);
   R.oct = (R.d.x < 0.0f ? 1u : 0u) | (R.d.y < 0.0f ? 2u : 0u) | (R.d.z < 0.0f ? 4u : 0u);
+  R.valid = R.d.x != 0.0f || R.d.y != 0.0f || R.d.z != 0.0f;
+  R.sheared = false;
+}
+
+// The triangle test's part for instance `inst` of the packed words (record rows at `r`): the
+// shear of Woop, Benthin and Wald (2013) for the object-space direction, and the error of the
+// f32 object-space origin against the f64 reference's (ray64's arithmetic over the same rows).
+__device__ __noinline__ void w8_shear(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray& R) {
   const float ax = fabsf(R.d.x), ay = fabsf(R.d.y), az = fabsf(R.d.z);
   const int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
   int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
@@ -151,8 +168,7 @@ RT_DEV void w8_setup(W8Ray& R) {
     kx = ky;
     ky = t;
   }
-  R.valid = dz != 0.0f;
-  const float sz = R.valid ? __frcp_rn(dz) : 0.0f;
+  const float sz = __frcp_rn(dz);  // dz != 0: the instance was entered with a valid direction
   const float sx = __fmul_rn(comp(kx), sz), sy = __fmul_rn(comp(ky), sz);
   // rows of the shear: M_x = e_kx - sx e_kz, M_y = e_ky - sy e_kz, M_z = sz e_kz
   auto row = [&](int one, float at_z) {
@@ -163,6 +179,17 @@ RT_DEV void w8_setup(W8Ray& R) {
   R.my = row(ky, -sy);
   R.mz = {kz == 0 ? sz : 0.0f, kz == 1 ? sz : 0.0f, kz == 2 ? sz : 0.0f};
   R.tscale = 8.0f * W8_U * fabsf(sz);
+  // the origin of the f64 reference (ray64's arithmetic), to bound the f32 origin's error
+  const double ox = world_o.x, oy = world_o.y, oz = world_o.z;
+  auto o64 = [&](size_t k) {
+    return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn((double)ldf(w, k), ox), __dmul_rn((double)ldf(w, k + 1), oy)),
+                               __dmul_rn((double)ldf(w, k + 2), oz)),
+                     (double)ldf(w, k + 3));
+  };
+  const double e = fmax(fmax(fabs(o64(r) - (double)R.o.x), fabs(o64(r + 4) - (double)R.o.y)),
+                        fabs(o64(r + 8) - (double)R.o.z));
+  R.oerr = e > 0.0 ? __double2float_ru(e) : 0.0f;
+  R.sheared = true;
 }
 
 // Projected vertex (Ax, Ay, Az): one fixed chain of operations per vertex. `m` keeps the
@@ -184,8 +211,9 @@ RT_DEV float w8_edge(float px, float py, float qx, float qy) {
 }
 
 // Watertight test. Returns 0 miss, 1 hit, 2 uncertain (near an edge: the caller re-tests in
-// f64). On hit / uncertain, t, u, v hold the f32 estimate (t may be outside the range).
-RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, float& v, float& dmax) {
+// f64). On hit / uncertain, t holds the f32 estimate (it may be outside the range); the
+// barycentrics of the final hit come from the f64 final pass.
+RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& dmax) {
   dmax = 0.0f;
   const F3 A = w8_project(R, v0, dmax), B = w8_project(R, v1, dmax), C = w8_project(R, v2, dmax);
   const float U = w8_edge(C.x, C.y, B.x, B.y);  // opposite v0
@@ -214,25 +242,51 @@ RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& u, 
   if (det == 0.0f) return sum > 0.0f ? 2 : 0;
   if (fabsf(U) <= lim || fabsf(V) <= lim || fabsf(W) <= lim) kind = 2;
   const float T = __fadd_rn(__fadd_rn(__fmul_rn(U, A.z), __fmul_rn(V, B.z)), __fmul_rn(W, C.z));
-  const float rd = __frcp_rn(det);
-  t = __fmul_rn(T, rd);
-  u = __fmul_rn(V, rd);
-  v = __fmul_rn(W, rd);
+  t = __fmul_rn(T, __frcp_rn(det));
   return kind;
+}
+
+// An uncertain candidate, decided in f64 (out of line: it is rare, and its doubles would
+// otherwise take registers from the walk). The candidate and, if the incumbent is still an f32
+// estimate, the incumbent are re-intersected with the f64 reference's arithmetic; the lower
+// (t, instance, triangle) wins. Returns true when the candidate is the new best.
+template <uint32_t LAYOUT>
+__device__ __noinline__ bool w8_resolve64(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t inst,
+                                          uint32_t tri, uint32_t ident, uint32_t ref, W8Best& best) {
+  double t64 = 0.0, u64 = 0.0, v64 = 0.0;
+  if (!mt64<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) return false;
+  if (best.hit && !best.has64) {
+    // the incumbent needs its f64 result too
+    const uint4 b2 = __ldg(V.tris + 3 * (size_t)best.tri + 2);
+    double bt, bu, bv;
+    if (mt64<LAYOUT>(w, best.inst, b2.z, ray, bt, bu, bv)) {
+      best.t64 = bt, best.t = (float)bt, best.has64 = true, best.band = 0.0f;
+    } else {
+      best.hit = false;  // the f32 estimate was a false hit: drop it
+    }
+  }
+  if (best.hit) {
+    const bool better = t64 < best.t64 || (t64 == best.t64 && (inst < best.inst || (inst == best.inst && ident < best.ident)));
+    if (!better) return false;
+  }
+  best.hit = true, best.has64 = true, best.t64 = t64, best.t = (float)t64, best.band = 0.0f;
+  best.inst = inst, best.tri = tri, best.ident = ident;
+  return true;
 }
 
 // Considers one candidate triangle; returns true when an any-hit query is satisfied.
 template <uint32_t LAYOUT, int AM, bool COUNT>
-RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const W8Ray& R, const Ray& ray, uint32_t inst,
+RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, W8Ray& R, const Ray& ray, uint32_t inst,
                          uint32_t tri, W8Best& best, unsigned long long* cnt, bool lane_any) {
   w8_count<COUNT>(cnt, W8C_TRIS);
+  if (!R.sheared) w8_shear(w, (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * inst, ray.o, R);
   const uint4 q0 = __ldg(V.tris + 3 * (size_t)tri), q1 = __ldg(V.tris + 3 * (size_t)tri + 1),
               q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
   const F3 v0 = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
   const F3 v1 = {__uint_as_float(q0.w), __uint_as_float(q1.x), __uint_as_float(q1.y)};
   const F3 v2 = {__uint_as_float(q1.z), __uint_as_float(q1.w), __uint_as_float(q2.x)};
-  float t, u, v, dmax;
-  const int kind = w8_triangle(R, v0, v1, v2, t, u, v, dmax);
+  float t, dmax;
+  const int kind = w8_triangle(R, v0, v1, v2, t, dmax);
   if (kind == 0) return false;
   const uint32_t ident = q2.y, ref = q2.z;
   const float tmin = ray.tmin, tmax = ray.tmax;
@@ -247,30 +301,13 @@ RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, const 
   }
   const bool uncertain = kind == 2 || !(t > tmin + band) || !(t < tmax - band) ||
                          (best.hit && t >= best.t - band - best.band);
-  double t64 = 0.0, u64 = 0.0, v64 = 0.0;
   if (uncertain) {
     w8_count<COUNT>(cnt, W8C_RETESTS);
-    if (!mt64<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) return false;
-    if (best.hit && !best.has64) {
-      // the incumbent needs its f64 result too
-      const uint4 b2 = __ldg(V.tris + 3 * (size_t)best.tri + 2);
-      double bt, bu, bv;
-      if (mt64<LAYOUT>(w, best.inst, b2.z, ray, bt, bu, bv)) {
-        best.t64 = bt, best.u = (float)bu, best.v = (float)bv, best.t = (float)bt, best.has64 = true, best.band = 0.0f;
-      } else {
-        best.hit = false;  // the f32 estimate was a false hit: drop it
-      }
-    }
-    if (best.hit) {
-      const bool better = t64 < best.t64 || (t64 == best.t64 && (inst < best.inst || (inst == best.inst && ident < best.ident)));
-      if (!better) return false;
-    }
-    best.hit = true, best.has64 = true, best.t64 = t64, best.t = (float)t64, best.u = (float)u64, best.v = (float)v64;
-    best.band = 0.0f;
+    if (!w8_resolve64<LAYOUT>(w, V, ray, inst, tri, ident, ref, best)) return false;
   } else {
-    best.hit = true, best.has64 = false, best.t = t, best.u = u, best.v = v, best.band = band;
+    best.hit = true, best.has64 = false, best.t = t, best.band = band;
+    best.inst = inst, best.tri = tri, best.ident = ident;
   }
-  best.inst = inst, best.tri = tri, best.ident = ident;
   return AM == 2 ? lane_any : AM == 1;
 }
 
@@ -368,7 +405,7 @@ template <uint32_t LAYOUT, int AM, bool COUNT, class Stack>
 RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, Stack& stack, DevStatus* st,
                     unsigned long long* cnt) {
   w8_count<COUNT>(cnt, W8C_NODES);
-  const W8Ray& R = L.R;
+  W8Ray& R = L.R;
   const uint4* np = V.nodes + 5 * (size_t)L.node;
   const uint4 a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
   const uint32_t imask = a0.w >> 24;
@@ -430,16 +467,6 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   const float r10 = ldf(w, r + 4), r11 = ldf(w, r + 5), r12 = ldf(w, r + 6), r13 = ldf(w, r + 7);
   const float r20 = ldf(w, r + 8), r21 = ldf(w, r + 9), r22 = ldf(w, r + 10), r23 = ldf(w, r + 11);
   L.R.o = {dot4p(r00, r01, r02, r03, L.ray.o), dot4p(r10, r11, r12, r13, L.ray.o), dot4p(r20, r21, r22, r23, L.ray.o)};
-  {  // the origin of the f64 reference (ray64's arithmetic), to bound the f32 origin's error
-    const double ox = L.ray.o.x, oy = L.ray.o.y, oz = L.ray.o.z;
-    auto o64 = [&](float a, float b, float c, float d) {
-      return __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(a, ox), __dmul_rn(b, oy)), __dmul_rn(c, oz)), (double)d);
-    };
-    const double ex = fabs(o64(r00, r01, r02, r03) - (double)L.R.o.x), ey = fabs(o64(r10, r11, r12, r13) - (double)L.R.o.y),
-                 ez = fabs(o64(r20, r21, r22, r23) - (double)L.R.o.z);
-    const double e = fmax(fmax(ex, ey), ez);
-    L.R.oerr = e > 0.0 ? __double2float_ru(e) : 0.0f;
-  }
   L.R.d = {dot3({r00, r01, r02}, L.ray.d), dot3({r10, r11, r12}, L.ray.d), dot3({r20, r21, r22}, L.ray.d)};
   w8_setup(L.R);
   if (!L.R.valid) return;
@@ -617,7 +644,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
       b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
-      b.inst = EMPTY, b.tri = 0, b.ident = 0, b.u = b.v = 0.0f;
+      b.inst = EMPTY, b.tri = 0, b.ident = 0;
       L.phase = 1;
       L.flat = 0;
       L.tsp = 0;
@@ -670,7 +697,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
 // depend on the visit order (conservative boxes, ties resolved in f64 on (t, instance,
 // triangle)), so each ray gets the hit the per-ray walk finds.
 template <uint32_t LAYOUT, int AM, int BLOCK, class Src>
-__global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
+__global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                            unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
   __shared__ uint2 warp_stack[BLOCK / 32][W8_STACK];
   uint2* stack = warp_stack[threadIdx.x >> 5];
@@ -690,7 +717,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8_packet(const 
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
       b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
-      b.inst = EMPTY, b.tri = 0, b.ident = 0, b.u = b.v = 0.0f;
+      b.inst = EMPTY, b.tri = 0, b.ident = 0;
     }
     for (uint32_t i = 0; i < count && __any_sync(0xffffffffu, live); ++i) {
       L.phase = 0;

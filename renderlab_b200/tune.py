@@ -10,8 +10,10 @@ Parameters searched (each candidate is one rt_plan, timed as a whole, sort inclu
 * wavefront width -- the refill threshold: how many lanes of a 32-wide warp must be idle before
   the warp takes more rays (1 keeps every lane busy; 32 hands out whole runs of 32 consecutive
   rays, which keeps a coherent batch's 8 x 4 tiles together);
-* sort key -- none, or a ray permutation by origin Morton code / octant + origin (rt_order_rays
-  over the plan's whole ray space, run inside the plan on every launch).
+* sort key -- none, or a ray permutation by origin Morton code / octant + origin / octahedral
+  direction cell + coarse origin (rt_order_rays over the plan's whole ray space, run inside the
+  plan on every launch). The direction key gathers rays toward one light from nearby points,
+  which lets the packet walk share their traversal.
 
 * stack -- for WIDE8's per-ray walk, where each lane keeps its node-group stack: 32 entries in
   local memory (cached by L1), or 16 in a shared-memory column of the block (only when the
@@ -31,7 +33,7 @@ from . import api as A
 
 KERNELS = ("plain", "fast", "wide8", "wide8p")
 REFILLS = (4, 8, 16, 32)
-ORDERS = ("none", "origin", "octant")
+ORDERS = ("none", "origin", "octant", "direction")
 STACKS = ("local", "shared")
 
 
