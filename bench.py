@@ -718,8 +718,10 @@ def run_ours(args):
     for g in wl.groups:
         batches = [(dev[i], wl.batches[i].mode) for i in g]
         if args.kernel == "auto":
-            heavy = len(g) > 8  # the many-batch launch runs for seconds: one timed launch a candidate
-            ch = T.tune(engine, scene, batches, flush=flush, reps=1 if heavy else 3, max_seconds=20.0)
+            heavy = len(g) > 8  # the many-batch launch runs for seconds: one timed launch a candidate,
+            # and no packet walk (its incoherent random rays would take many seconds a trial)
+            ch = T.tune(engine, scene, batches, flush=flush, reps=1 if heavy else 3, max_seconds=20.0,
+                        kernels=("plain", "fast", "wide8") if heavy else T.KERNELS)
             plans.append(ch.plan)
             tables.append(ch.table()[:6])
         elif args.kernel == "plain":
@@ -888,6 +890,17 @@ def run_ours(args):
                          "not the limit; traffic is ncu's DRAM bytes per ray on this launch, scaled to its rays")
         if all(x is not None for x in group_bytes):
             roof["step_achieved"] = sum(group_bytes) / (ms * 1e-3) / 1e9
+        # The L2 ceiling beside the HBM one: this device's read bandwidth over a 48 MiB buffer
+        # (L2-resident) and a 4 GiB one (HBM), measured here with rt_read_bandwidth.
+        try:
+            l2 = engine.read_bandwidth(48 << 20, 50)
+            hbm_read = engine.read_bandwidth(4 << 30, 3)
+            roof["l2"] = dict(peak=l2, unit="GB/s", frac=achieved / l2, hbm_read_peak=hbm_read,
+                              note="read bandwidth measured in this run (16-byte loads, L1 bypassed) over a "
+                                   "48 MiB buffer (L2) and a 4 GiB buffer (HBM); the algorithmic bytes are "
+                                   "served by L1 and L2 when the scene fits L2, so this is the tighter ceiling")
+        except Exception as exc:  # the probe needs 4 GiB free
+            roof["l2"] = dict(peak=None, note=f"not measured: {exc}")
     def launches(g, p):  # traversal kernels (and ray-key kernels) a step launches
         if p is None or p.desc["kernel"] == "plain":
             return sum(1 for i in g if len(wl.batches[i].rays))

@@ -59,8 +59,8 @@ typedef enum rt_kernel {
   RT_KERNEL_PLAIN = 0,
   RT_KERNEL_FAST = 1,
   RT_KERNEL_WIDE8 = 2,
-  RT_KERNEL_WIDE8_PACKET = 3 /* WIDE8 walked by warp-wide packets of 32 consecutive rays, for coherent
-                                batches over flat instance lists (no top level); WIDE8's results */
+  RT_KERNEL_WIDE8_PACKET = 3 /* WIDE8 walked by warp-wide packets of 32 consecutive rays (top level and
+                                BLAS), for coherent batches; WIDE8's results */
 } rt_kernel;
 
 /* One ray, 32 bytes: origin, tmin, direction (need not be unit length), tmax. */
@@ -355,6 +355,13 @@ rt_status rt_ctx_reserve(rt_ctx* ctx, uint32_t max_rays);
  * the reference traversal visits). Synchronous. */
 rt_status rt_trace_counted(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel kernel,
                            const rt_ray* d_rays, void* d_hits, uint32_t n, uint64_t counts[8]);
+
+/* Read bandwidth of the context's device in GB/s, for the traversal's roofline (no counterpart in
+ * the reference): 16-byte loads that bypass L1 stream `reps` times over a device buffer of
+ * `bytes` (at least 1 MiB), timed with CUDA events after one warm pass. A buffer well inside the
+ * 126 MB L2 measures L2's read bandwidth, one far larger than L2 measures HBM's. Synchronous;
+ * allocates and frees the buffer. */
+rt_status rt_read_bandwidth(rt_ctx* ctx, uint64_t bytes, uint32_t reps, double* gbs);
 
 /* ---- allocation-free traversal ----
  * No counterpart in the reference: renderlab always traverses inside its own renderer.

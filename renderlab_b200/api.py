@@ -104,7 +104,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
            "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_trace_gi_lights", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_fail_next", "rt_server_destroy",
-           "rt_trace_static", "rt_trace_static_stack_drops", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
+           "rt_trace_static", "rt_trace_static_stack_drops", "rt_read_bandwidth", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
            "rt_scene_move_instances", "rt_blas_build", "rt_blas_build_device", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
            "rt_blas_free", "rt_pack_scene", "rt_tlas_build", "rt_tlas_build_device", "rt_tlas_refit", "rt_blas_positions",
            "rt_blas_encode_rlb", "rt_rlb_decode", "rt_rnf_decode", "rt_rnf_info", "rt_rnf_mesh",
@@ -174,6 +174,7 @@ def lib() -> ctypes.CDLL:
     L.rt_server_destroy.argtypes = [_vp]
     L.rt_trace_static.argtypes = [ctypes.c_int, _vp, ctypes.c_size_t, ctypes.c_int, _vp, _vp, ctypes.c_uint32, _vp]
     L.rt_trace_static_stack_drops.argtypes = [_vp, ctypes.POINTER(ctypes.c_uint64)]
+    L.rt_read_bandwidth.argtypes = [_vp, ctypes.c_uint64, ctypes.c_uint32, ctypes.POINTER(ctypes.c_double)]
     L.rt_trace_counted.argtypes = [_vp, _vp, ctypes.c_int, ctypes.c_int, _vp, _vp, ctypes.c_uint32,
                                    ctypes.POINTER(ctypes.c_uint64)]
     L.rt_blas_build.argtypes = [_f32p, ctypes.c_uint32, _u32p, ctypes.c_uint32, ctypes.c_uint32, ctypes.POINTER(_vp)]
@@ -780,6 +781,13 @@ class Engine:
         self._check(lib().rt_trace_counted(self.ctx, scene.handle, mode, KERNELS[kernel], rays.data_ptr(),
                                            hits.data_ptr(), n, out))
         return dict(zip(self.COUNTERS, map(int, out)))
+
+    def read_bandwidth(self, nbytes: int, reps: int = 20) -> float:
+        """rt_read_bandwidth: GB/s of 16-byte loads (L1 bypassed) over an `nbytes` device buffer --
+        L2's read bandwidth for buffers well inside L2, HBM's for buffers far larger."""
+        out = ctypes.c_double(0.0)
+        self._check(lib().rt_read_bandwidth(self.ctx, int(nbytes), int(reps), ctypes.byref(out)))
+        return out.value
 
     def reserve(self, max_rays: int):
         self._check(lib().rt_ctx_reserve(self.ctx, max_rays))

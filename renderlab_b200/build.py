@@ -29,7 +29,7 @@ NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompil
 CXX_FLAGS = ["-O2", "-std=c++17", "-fPIC", "-ffp-contract=off", "-fno-fast-math", "-Wall", "-Wextra",
              "-Wno-unused-parameter", "-I", str(ROOT / "include")]
 
-CU_SOURCES = ["rt_api.cu", "kernels_plain.cu", "kernels_fast.cu", "kernels_wide8.cu", "kernels_order.cu", "batches.cu", "serve.cu", "refit.cu", "kernels_cells.cu", "trace_static.cu", "move.cu", "blas_build.cu", "tlas_build.cu"]
+CU_SOURCES = ["rt_api.cu", "kernels_plain.cu", "kernels_fast.cu", "kernels_wide8.cu", "kernels_order.cu", "batches.cu", "serve.cu", "refit.cu", "kernels_cells.cu", "trace_static.cu", "move.cu", "blas_build.cu", "tlas_build.cu", "diag.cu"]
 CPP_SOURCES = ["host/blas.cpp", "host/tlas.cpp", "host/pack.cpp", "host/validate.cpp", "host/wide8.cpp", "host/cooked.cpp", "host/wide8_check.cpp"]
 
 

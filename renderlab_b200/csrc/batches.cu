@@ -24,8 +24,6 @@ rt_status make_table(rt_ctx* ctx, const rt_scene* scene, rt_kernel kernel, const
     return fail(ctx, RT_ERR_UNSUPPORTED, "kernel %d is not available", (int)kernel);
   if (scene->layout == RT_LAYOUT_REFLECTION_BVH2 && kernel != RT_KERNEL_PLAIN)
     return fail(ctx, RT_ERR_UNSUPPORTED, "the legacy BVH2 layout is traced by the PLAIN kernel");
-  if (kernel == RT_KERNEL_WIDE8_PACKET && scene->info.top != 0)
-    return fail(ctx, RT_ERR_UNSUPPORTED, "the packet walk takes flat instance lists only");
   if (wide && !scene->d_wide8)
     return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
   if (n && !b) return fail(ctx, RT_ERR_INVALID_ARG, "null batch array");

@@ -688,21 +688,77 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
   }
 }
 
-// Packet walk, for coherent batches over flat instance lists: a warp takes 32 consecutive rays and
-// walks ONE 8-wide traversal for all of them. A node's child is visited when any lane's ray meets
-// its box, in the first entering lane's octant order, so every lane reads the same node (one
-// broadcast load) and no lane diverges on the walk; the traversal stack is the warp's, in shared
-// memory. Each lane still tests its own ray against every visited node's boxes (its own hits and
-// closest-hit bound) and against the triangles of the leaves its ray meets. WIDE8's results do not
-// depend on the visit order (conservative boxes, ties resolved in f64 on (t, instance,
-// triangle)), so each ray gets the hit the per-ray walk finds.
+// One top-level node of the packet walk: each live lane computes its four slab entries against its
+// own bound (the per-ray walk's, from its best hit); a child is visited when any lane meets it,
+// nearest (over the lanes' entries) first. Lane 0 pushes onto the warp's top stack; every lane
+// returns the stack's new depth.
+RT_DEV uint32_t w8_packet_top(const uint32_t* __restrict__ w, size_t n, const W8Lane& L, bool live, uint32_t* tstack,
+                              uint32_t sp, DevStatus* st) {
+  uint32_t key[4], ids[4];
+  const W8Best& b = L.best;
+  const float bound = b.hit ? b.t + 2.0f * b.band + 2.0f * W8_TIE * b.t : b.t;
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    ids[c] = ld(w, n + 24 + c);
+    uint32_t k = 0xffffffffu;  // no lane meets the child
+    if (live && ids[c] != EMPTY) {
+      const F3& o = L.ray.o;
+      const F3& inv = L.world_inv;
+      const float ax = mul(sub(ldf(w, n + c), o.x), inv.x), bx = mul(sub(ldf(w, n + 12 + c), o.x), inv.x);
+      const float ay = mul(sub(ldf(w, n + 4 + c), o.y), inv.y), by = mul(sub(ldf(w, n + 16 + c), o.y), inv.y);
+      const float az = mul(sub(ldf(w, n + 8 + c), o.z), inv.z), bz = mul(sub(ldf(w, n + 20 + c), o.z), inv.z);
+      const float near = fmaxf(fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz)), L.ray.tmin);
+      const float far = fminf(fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz)), bound);
+      if (near <= far) {  // an order-preserving key of the entry distance
+        const uint32_t u = __float_as_uint(near);
+        k = (u >> 31) ? ~u : (u | 0x80000000u);
+        k = k == 0xffffffffu ? 0xfffffffeu : k;
+      }
+    }
+    key[c] = __reduce_min_sync(0xffffffffu, k);
+  }
+#define RT_SW(a, b)                                                     \
+  if (key[b] < key[a]) {                                                \
+    uint32_t x = key[a]; key[a] = key[b]; key[b] = x;                   \
+    x = ids[a]; ids[a] = ids[b]; ids[b] = x;                            \
+  }
+  RT_SW(0, 1) RT_SW(2, 3) RT_SW(0, 2) RT_SW(1, 3) RT_SW(1, 2)
+#undef RT_SW
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int c = 3; c >= 0; --c) {  // far to near: the nearest is popped first
+    if (key[c] == 0xffffffffu) continue;
+    if (sp < STACK) {
+      if (lane == 0) tstack[sp] = ids[c];
+      ++sp;
+    } else if (lane == 0) {
+      atomicAdd(&st->stack_drops, 1ull);
+    }
+  }
+  __syncwarp();
+  return sp;
+}
+
+// Packet walk, for coherent batches: a warp takes 32 consecutive rays and walks ONE traversal for
+// all of them -- the top level's BVH4 (or the flat instance list) and each entered instance's
+// 8-wide BLAS. A node's child is visited when any lane's ray meets its box, in the first entering
+// lane's octant order (top-level nodes: nearest entry over the lanes first), so every lane reads
+// the same node (one broadcast load) and no lane diverges on the walk; the traversal stacks are
+// the warp's, in shared memory. Each lane still tests its own ray against every visited node's
+// boxes (its own hits and closest-hit bound), enters only the instances whose world box its ray
+// meets, and tests the triangles of the leaves its ray meets. WIDE8's results do not depend on
+// the visit order (conservative boxes, ties resolved in f64 on (t, instance, triangle)), so each
+// ray gets the hit the per-ray walk finds.
 template <uint32_t LAYOUT, int AM, int BLOCK, class Src>
 __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                            unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
   __shared__ uint2 warp_stack[BLOCK / 32][W8_STACK];
+  __shared__ uint32_t warp_top[BLOCK / 32][STACK];
   uint2* stack = warp_stack[threadIdx.x >> 5];
+  uint32_t* tstack = warp_top[threadIdx.x >> 5];
   const int lane = threadIdx.x & 31;
-  const uint32_t count = ld(w, 0);
+  const uint32_t count = ld(w, 0), top = ld(w, 1), root = ld(w, 2);
+  const size_t top_base = LAYOUT == 0 ? top : (top & ~3u);
   for (;;) {
     uint32_t base = 0;
     if (lane == 0) base = atomicAdd(counter, 32u);
@@ -719,7 +775,27 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
       b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
       b.inst = EMPTY, b.tri = 0, b.ident = 0;
     }
-    for (uint32_t i = 0; i < count && __any_sync(0xffffffffu, live); ++i) {
+    uint32_t flat = 0, tsp = 0;
+    if (top != 0 && count != 0) {
+      if (lane == 0) tstack[0] = root;
+      __syncwarp();
+      tsp = 1;
+    }
+    while (__any_sync(0xffffffffu, live)) {
+      uint32_t i;  // the next instance the warp tries (uniform)
+      if (top == 0) {
+        if (flat >= count) break;
+        i = flat++;
+      } else {
+        if (tsp == 0) break;
+        const uint32_t item = tstack[--tsp];
+        __syncwarp();  // every lane has read the entry before lane 0 may overwrite it
+        if (!(item & LEAF)) {
+          tsp = w8_packet_top(w, top_base + (size_t)item * 32, L, live, tstack, tsp, st);
+          continue;
+        }
+        i = item & ~LEAF;
+      }
       L.phase = 0;
       if (live) w8_enter<LAYOUT, AM, false>(w, V, L, i, nullptr);
       bool in = L.phase == 2;

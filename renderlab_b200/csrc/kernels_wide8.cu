@@ -175,7 +175,7 @@ cudaError_t launch_wide8_packet(const SceneView& s, uint32_t mode, const float4*
                                 uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream) {
   if (n == 0) return cudaSuccess;
   rtk::W8View v;
-  if (!view_of(s, v) || s.top != 0) return cudaErrorInvalidValue;
+  if (!view_of(s, v)) return cudaErrorInvalidValue;
   using rtk::OneBatch;
   const OneBatch src{rays, order, hits};
   cudaError_t e;
@@ -194,7 +194,7 @@ cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntr
                                         rtk::DevStatus* st, cudaStream_t stream, int uniform_mode) {
   if (total == 0) return cudaSuccess;
   rtk::W8View v;
-  if (!view_of(s, v) || s.top != 0) return cudaErrorInvalidValue;
+  if (!view_of(s, v)) return cudaErrorInvalidValue;
   using rtk::ManyBatches;
   const ManyBatches src{table, entries, order};
 #define RT_W8P(L, AM) run_packet(rtk::k_wide8_packet<L, AM, W8_BLOCK, ManyBatches>, s.words, v, src, counter, total, st, stream)

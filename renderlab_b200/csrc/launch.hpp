@@ -50,8 +50,8 @@ cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* tabl
 // WIDE8 with per-event device counters (rtk::W8Count order) accumulated into cnt[8].
 cudaError_t count_wide8(const SceneView& s, uint32_t mode, const float4* rays, void* hits, uint32_t n,
                         unsigned int* counter, rtk::DevStatus* st, unsigned long long* cnt, cudaStream_t stream);
-// WIDE8 walked by warp-wide packets of 32 consecutive rays (flat instance lists only: s.top == 0);
-// the same results as launch_wide8.
+// WIDE8 walked by warp-wide packets of 32 consecutive rays (top level or flat instance list); the
+// same results as launch_wide8.
 cudaError_t launch_wide8_packet(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                                 uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream);
 cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries,

@@ -50,7 +50,6 @@ rt_status dispatch(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_kernel k
     case RT_KERNEL_WIDE8_PACKET:
       if (!scene->d_wide8)
         return fail(ctx, RT_ERR_UNSUPPORTED, "the WIDE8 kernel needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first");
-      if (scene->info.top != 0) return fail(ctx, RT_ERR_UNSUPPORTED, "the packet walk takes flat instance lists only");
       e = rtl::launch_wide8_packet(v, (uint32_t)mode, r, order, hits, n,
                                    ctx->d_counters + (ctx->counter_seq++ % COUNTER_SLOTS), ctx->d_status, stream);
       break;

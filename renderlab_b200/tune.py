@@ -6,7 +6,7 @@ Parameters searched (each candidate is one rt_plan, timed as a whole, sort inclu
 * kernel -- PLAIN (one thread per ray, a launch per batch), FAST (persistent warps over the
   BVH4-Q8, bit-exact with the reference loop like PLAIN) or WIDE8 (8-wide compressed nodes,
   watertight f32 test with f64 re-tests) or WIDE8 walked by warp-wide packets of 32 rays ("wide8p":
-  the same results; flat instance lists only);
+  the same results, the top level walked by the packet too);
 * wavefront width -- the refill threshold: how many lanes of a 32-wide warp must be idle before
   the warp takes more rays (1 keeps every lane busy; 32 hands out whole runs of 32 consecutive
   rays, which keeps a coherent batch's 8 x 4 tiles together);

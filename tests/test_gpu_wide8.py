@@ -169,19 +169,32 @@ def test_wide8_refuses_blas_beyond_its_decode_range(engine):
         scene.release()
 
 
-def test_packet_walk_needs_a_flat_instance_list(engine):
-    """The packet walk shares one traversal between 32 rays and covers flat instance lists; a
-    scene with a top level is refused, not walked wrongly."""
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_packet_walk_over_a_top_level(engine, layout):
+    """The packet walk also walks a scene's top level (900 cube instances, some casting no
+    shadow): per ray it returns the per-ray walk's records exactly -- closest hits, and both
+    any-hit modes -- and the FP64 oracle's hit ids, for coherent camera rays and random rays."""
     import torch
-    mesh, inst = S.cubes_instanced(8)
-    w = product_words(A.LAYOUT_REFLECTION, [mesh], inst)
+    mesh, inst = S.cubes_instanced(30)
+    inst.casts = (np.arange(len(inst)) % 5) != 2
+    w = product_words(layout, [mesh], inst)
     assert w[1] != 0
-    scene = engine.upload(A.LAYOUT_REFLECTION, w)
+    scene = engine.upload(layout, w)
     try:
         scene.prepare("wide8")
-        rays = torch.from_numpy(H.small_cubes(8, 16, 16)[1]).cuda()
-        with pytest.raises(A.RtError, match="UNSUPPORTED"):
-            engine.trace(scene, rays, A.CLOSEST, "wide8p")
+        cam = H.small_cubes(30, 128, 96)[1]
+        rnd = H.random_rays(8_000, -30.0, 30.0, seed=8, tmax=200.0)
+        for rays in (cam, rnd):
+            d = torch.from_numpy(rays).cuda()
+            for mode in (A.CLOSEST, A.ANY_SKY, A.ANY_CASTERS):
+                a = engine.trace(scene, d, mode, "wide8")
+                b = engine.trace(scene, d, mode, "wide8p")
+                torch.cuda.synchronize()
+                assert torch.equal(a, b), f"mode {mode}: {(a != b).sum().item()} words differ"
+            got = engine.trace(scene, d, A.CLOSEST, "wide8p").cpu().numpy().view(np.uint32)
+            ref, ident = O.fp64_trace(w, rays, layout)
+            check_closest(layout, got, ref, ident, "packet walk over a top level")
+        assert (got[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)).mean() > 0.05
     finally:
         scene.release()
 
