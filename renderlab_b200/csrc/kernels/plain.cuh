@@ -153,14 +153,21 @@ RT_DEV void top_step(const uint32_t* __restrict__ w, size_t n, const Ray& ray, F
                      uint32_t* stack, uint32_t& sp, DevStatus* st) {
   float dist[4];
   uint32_t ids[4];
+  // the node's seven 16-byte rows: lo x, lo y, lo z, hi x, hi y, hi z (four children each), ids
+  const uint4 lx = ld4u(w, n), ly = ld4u(w, n + 4), lz = ld4u(w, n + 8);
+  const uint4 hx = ld4u(w, n + 12), hy = ld4u(w, n + 16), hz = ld4u(w, n + 20), id4 = ld4u(w, n + 24);
+  auto at = [](const uint4& q, int c) { return c == 0 ? q.x : (c == 1 ? q.y : (c == 2 ? q.z : q.w)); };
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    const float ax = mul(sub(ldf(w, n + c), ray.o.x), world_inv.x), bx = mul(sub(ldf(w, n + 12 + c), ray.o.x), world_inv.x);
-    const float ay = mul(sub(ldf(w, n + 4 + c), ray.o.y), world_inv.y), by = mul(sub(ldf(w, n + 16 + c), ray.o.y), world_inv.y);
-    const float az = mul(sub(ldf(w, n + 8 + c), ray.o.z), world_inv.z), bz = mul(sub(ldf(w, n + 20 + c), ray.o.z), world_inv.z);
+    const float ax = mul(sub(__uint_as_float(at(lx, c)), ray.o.x), world_inv.x),
+                bx = mul(sub(__uint_as_float(at(hx, c)), ray.o.x), world_inv.x);
+    const float ay = mul(sub(__uint_as_float(at(ly, c)), ray.o.y), world_inv.y),
+                by = mul(sub(__uint_as_float(at(hy, c)), ray.o.y), world_inv.y);
+    const float az = mul(sub(__uint_as_float(at(lz, c)), ray.o.z), world_inv.z),
+                bz = mul(sub(__uint_as_float(at(hz, c)), ray.o.z), world_inv.z);
     const float near = fmaxf(fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz)), ray.tmin);
     const float far = fminf(fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz)), bound);
-    ids[c] = ld(w, n + 24 + c);
+    ids[c] = at(id4, c);
     dist[c] = (near <= far && ids[c] != EMPTY) ? near : BIG;
   }
 #define RT_SW(a, b)                                      \

@@ -697,16 +697,19 @@ RT_DEV uint32_t w8_packet_top(const uint32_t* __restrict__ w, size_t n, const W8
   uint32_t key[4], ids[4];
   const W8Best& b = L.best;
   const float bound = b.hit ? b.t + 2.0f * b.band + 2.0f * W8_TIE * b.t : b.t;
+  const uint4 lx = ld4u(w, n), ly = ld4u(w, n + 4), lz = ld4u(w, n + 8);
+  const uint4 hx = ld4u(w, n + 12), hy = ld4u(w, n + 16), hz = ld4u(w, n + 20), id4 = ld4u(w, n + 24);
+  auto at = [](const uint4& q, int c) { return c == 0 ? q.x : (c == 1 ? q.y : (c == 2 ? q.z : q.w)); };
 #pragma unroll
   for (int c = 0; c < 4; ++c) {
-    ids[c] = ld(w, n + 24 + c);
+    ids[c] = at(id4, c);
     uint32_t k = 0xffffffffu;  // no lane meets the child
     if (live && ids[c] != EMPTY) {
       const F3& o = L.ray.o;
       const F3& inv = L.world_inv;
-      const float ax = mul(sub(ldf(w, n + c), o.x), inv.x), bx = mul(sub(ldf(w, n + 12 + c), o.x), inv.x);
-      const float ay = mul(sub(ldf(w, n + 4 + c), o.y), inv.y), by = mul(sub(ldf(w, n + 16 + c), o.y), inv.y);
-      const float az = mul(sub(ldf(w, n + 8 + c), o.z), inv.z), bz = mul(sub(ldf(w, n + 20 + c), o.z), inv.z);
+      const float ax = mul(sub(__uint_as_float(at(lx, c)), o.x), inv.x), bx = mul(sub(__uint_as_float(at(hx, c)), o.x), inv.x);
+      const float ay = mul(sub(__uint_as_float(at(ly, c)), o.y), inv.y), by = mul(sub(__uint_as_float(at(hy, c)), o.y), inv.y);
+      const float az = mul(sub(__uint_as_float(at(lz, c)), o.z), inv.z), bz = mul(sub(__uint_as_float(at(hz, c)), o.z), inv.z);
       const float near = fmaxf(fmaxf(fmaxf(fminf(ax, bx), fminf(ay, by)), fminf(az, bz)), L.ray.tmin);
       const float far = fminf(fminf(fminf(fmaxf(ax, bx), fmaxf(ay, by)), fmaxf(az, bz)), bound);
       if (near <= far) {  // an order-preserving key of the entry distance
