@@ -454,18 +454,26 @@ RT_DEV bool w8_next(W8Lane& L, Stack& stack) {
 
 // Enters instance i when its world box survives; sets up the object-space ray.
 template <uint32_t LAYOUT, int AM, bool COUNT>
-RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i, unsigned long long* cnt) {
-  const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;
+// `from_top`: the instance comes from a top-level leaf, whose box the walk has just tested. That
+// box is the instance's world box, so its test here could only pass: the walk skips it (WIDE8's
+// results do not depend on which extra instances it enters, only its work does). A flat instance
+// list has no such test, so there the world box is tested here.
+RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i, unsigned long long* cnt,
+                     bool from_top) {
+  const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;  // 16-byte aligned records
   if (any_of<AM>(L) && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
   w8_count<COUNT>(cnt, W8C_INSTANCE_TESTS);
-  const W8Best& best = L.best;
-  const float bound = best.hit ? best.t + 2.0f * best.band + 2.0f * W8_TIE * best.t : L.ray.tmax;
-  if (!(slab_near(L.ray.o, L.world_inv, ld3(w, r + 12), ld3(w, r + 15), L.ray.tmin, bound) <= bound)) return;
+  if (!from_top) {
+    const W8Best& best = L.best;
+    const float bound = best.hit ? best.t + 2.0f * best.band + 2.0f * W8_TIE * best.t : L.ray.tmax;
+    if (!(slab_near(L.ray.o, L.world_inv, ld3(w, r + 12), ld3(w, r + 15), L.ray.tmin, bound) <= bound)) return;
+  }
   const uint32_t root = __ldg(V.inst + 2 * (size_t)i);
   if (root == EMPTY) return;
-  const float r00 = ldf(w, r), r01 = ldf(w, r + 1), r02 = ldf(w, r + 2), r03 = ldf(w, r + 3);
-  const float r10 = ldf(w, r + 4), r11 = ldf(w, r + 5), r12 = ldf(w, r + 6), r13 = ldf(w, r + 7);
-  const float r20 = ldf(w, r + 8), r21 = ldf(w, r + 9), r22 = ldf(w, r + 10), r23 = ldf(w, r + 11);
+  const uint4 q0 = ld4(w, r), q1 = ld4(w, r + 4), q2 = ld4(w, r + 8);
+  const float r00 = __uint_as_float(q0.x), r01 = __uint_as_float(q0.y), r02 = __uint_as_float(q0.z), r03 = __uint_as_float(q0.w);
+  const float r10 = __uint_as_float(q1.x), r11 = __uint_as_float(q1.y), r12 = __uint_as_float(q1.z), r13 = __uint_as_float(q1.w);
+  const float r20 = __uint_as_float(q2.x), r21 = __uint_as_float(q2.y), r22 = __uint_as_float(q2.z), r23 = __uint_as_float(q2.w);
   L.R.o = {dot4p(r00, r01, r02, r03, L.ray.o), dot4p(r10, r11, r12, r13, L.ray.o), dot4p(r20, r21, r22, r23, L.ray.o)};
   L.R.d = {dot3({r00, r01, r02}, L.ray.d), dot3({r10, r11, r12}, L.ray.d), dot3({r20, r21, r22}, L.ray.d)};
   w8_setup(L.R);
@@ -668,7 +676,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
           w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
           continue;
         }
-        w8_enter<LAYOUT, AM, COUNT>(w, V, L, L.flat++, cnt);
+        w8_enter<LAYOUT, AM, COUNT>(w, V, L, L.flat++, cnt, false);
         continue;
       }
       if (L.tsp == 0) {
@@ -677,7 +685,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       }
       const uint32_t item = tstack[--L.tsp];
       if (item & LEAF) {
-        w8_enter<LAYOUT, AM, COUNT>(w, V, L, item & ~LEAF, cnt);
+        w8_enter<LAYOUT, AM, COUNT>(w, V, L, item & ~LEAF, cnt, true);
         continue;
       }
       const W8Best& b = L.best;
@@ -800,7 +808,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
         i = item & ~LEAF;
       }
       L.phase = 0;
-      if (live) w8_enter<LAYOUT, AM, false>(w, V, L, i, nullptr);
+      if (live) w8_enter<LAYOUT, AM, false>(w, V, L, i, nullptr, false);
       bool in = L.phase == 2;
       const unsigned entering = __ballot_sync(0xffffffffu, in);
       if (!entering) continue;
