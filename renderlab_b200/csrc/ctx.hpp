@@ -35,6 +35,14 @@ struct rt_scene {
   size_t wide8_bytes = 0;
   size_t w8_nodes_at = 0, w8_tris_at = 0, w8_inst_at = 0;
   uint32_t w8_depth = 0;  // levels of the deepest 8-wide BLAS
+  // The WIDE8 walk's 8-wide top level over the instance world boxes (its own allocation: nodes,
+  // then instance items). Built by rt_scene_prepare when the packed scene has a top level; a
+  // rewrite of the records or the top level makes it stale, and the walk then uses the packed
+  // BVH4 top level until rt_scene_prepare builds it again.
+  void* d_w8_top = nullptr;
+  size_t w8_top_bytes = 0, w8_top_items_at = 0;
+  uint32_t w8_top_nodes = 0;
+  bool w8_top_valid = false;
   std::map<uint32_t, RefitLevels> refit;  // by the BLAS's node base word
   // rt_scene_move_instances: staging for the moved instances and mesh boxes, and the top level's
   // nodes grouped by height (deepest last), kept until a rebuild changes the tree.
@@ -144,6 +152,9 @@ inline rtl::SceneView view_of(const rt_scene* s) {
   v.wide8_bytes = s->wide8_bytes;
   v.w8_nodes_at = s->w8_nodes_at, v.w8_tris_at = s->w8_tris_at, v.w8_inst_at = s->w8_inst_at;
   v.w8_depth = s->w8_depth;
+  v.w8_top = s->w8_top_valid ? s->d_w8_top : nullptr;
+  v.w8_top_nodes = s->w8_top_valid ? s->w8_top_nodes : 0;
+  v.w8_top_items_at = s->w8_top_items_at;
   return v;
 }
 

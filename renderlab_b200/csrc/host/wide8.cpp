@@ -36,27 +36,34 @@ struct BNode {
   uint32_t first, count;  // count > 0: leaf over refs[first, first + count)
 };
 
+// Binned-SAH binary tree over primitive boxes: triangles for a BLAS, instance world boxes for a
+// top level.
 class Binary {
  public:
-  explicit Binary(const std::vector<SrcTri>& t) : tris_(t) {
-    const size_t n = t.size();
-    box_.resize(n);
-    cen_.resize(3 * n);
-    for (size_t i = 0; i < n; ++i) {
+  explicit Binary(const std::vector<SrcTri>& t) {
+    std::vector<Aabb> boxes(t.size());
+    for (size_t i = 0; i < t.size(); ++i) {
       Aabb b = Aabb::empty();
       for (int k = 0; k < 3; ++k) b.grow(&t[i].v[3 * k]);
-      box_[i] = b;
-      for (int a = 0; a < 3; ++a) cen_[3 * i + a] = 0.5f * (b.lo[a] + b.hi[a]);
+      boxes[i] = b;
     }
-    ref_.resize(n);
-    std::iota(ref_.begin(), ref_.end(), 0u);
+    init(std::move(boxes));
   }
+  explicit Binary(std::vector<Aabb> boxes) { init(std::move(boxes)); }
   int build() { return node(0, (uint32_t)ref_.size()); }
   const std::vector<BNode>& nodes() const { return nodes_; }
   const std::vector<uint32_t>& refs() const { return ref_; }
 
  private:
-  const std::vector<SrcTri>& tris_;
+  void init(std::vector<Aabb> boxes) {
+    box_ = std::move(boxes);
+    const size_t n = box_.size();
+    cen_.resize(3 * n);
+    for (size_t i = 0; i < n; ++i)
+      for (int a = 0; a < 3; ++a) cen_[3 * i + a] = 0.5f * (box_[i].lo[a] + box_[i].hi[a]);
+    ref_.resize(n);
+    std::iota(ref_.begin(), ref_.end(), 0u);
+  }
   std::vector<Aabb> box_;
   std::vector<float> cen_;
   std::vector<uint32_t> ref_;
@@ -220,26 +227,24 @@ class Collapse {
   }
 };
 
-}  // namespace
-
-void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
-  out = Wide8Blas{};
-  if (tris.empty()) return;
-  Binary bin(tris);
-  const int broot = bin.build();
-  std::vector<BNode> bn = bin.nodes();
-  const auto& refs = bin.refs();
+// The 8-wide nodes of a binary tree (root `broot`), in breadth-first order from node 0: the SAH-
+// optimal collapse, octant slots, child boxes quantised outward. A leaf slot's primitives are
+// appended by `leaf(ref)` (its first one at index `leaf.base()` when the node is written), so the
+// same emission serves triangle BLASes and instance top levels.
+template <class Leaf>
+void emit_wide8(std::vector<BNode>& bn, int broot, const std::vector<uint32_t>& refs, std::vector<uint32_t>& nodes,
+                int& max_exponent, uint32_t& depth, Leaf& leaf) {
   const Collapse plan(bn);
   struct Task { uint32_t wide; int b; uint32_t level; };
   std::deque<Task> queue;
-  out.nodes.resize(W8_NODE_WORDS, 0);
+  nodes.resize(W8_NODE_WORDS, 0);
   queue.push_back({0, broot, 1});
   while (!queue.empty()) {
     const Task task = queue.front();
     queue.pop_front();
-    out.depth = std::max(out.depth, task.level);
+    depth = std::max(depth, task.level);
     std::vector<int> kids;
-    if (bn[task.b].count > 0) kids.push_back(task.b);  // a BLAS of one leaf
+    if (bn[task.b].count > 0) kids.push_back(task.b);  // a tree of one leaf
     else kids = plan.children(task.b);
     // octant slots: greedy on the children's centre offsets from the node centre
     Aabb nb = Aabb::empty();
@@ -271,17 +276,15 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
         slot_of[bsl] = bk;
       }
     }
-    uint32_t* w = &out.nodes[(size_t)task.wide * W8_NODE_WORDS];
     // scale
     float p[3];
     int ex[3];
     for (int a = 0; a < 3; ++a) {
       p[a] = nb.lo[a];
       ex[a] = scale_exponent((double)nb.hi[a] - (double)p[a]);
-      out.max_exponent = std::max(out.max_exponent, ex[a]);
+      max_exponent = std::max(max_exponent, ex[a]);
     }
-    uint32_t imask = 0, child_base = (uint32_t)(out.nodes.size() / W8_NODE_WORDS),
-             tri_base = (uint32_t)(out.tris.size() / W8_TRI_WORDS);
+    uint32_t imask = 0, child_base = (uint32_t)(nodes.size() / W8_NODE_WORDS), leaf_base = leaf.base();
     uint8_t meta[8] = {}, q[6][8] = {};
     uint32_t inner = 0, offset = 0;
     for (int s = 0; s < 8; ++s) {
@@ -301,22 +304,16 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
         ++inner;
       } else {
         meta[s] = (uint8_t)(k.count << 5 | offset);
-        for (uint32_t t = 0; t < k.count; ++t) {
-          const SrcTri& src = tris[refs[k.first + t]];
-          for (int j = 0; j < 9; ++j) out.tris.push_back(as_bits(src.v[j]));
-          out.tris.push_back(src.ident);
-          out.tris.push_back(src.ref);
-          out.tris.push_back(0);
-        }
+        for (uint32_t t = 0; t < k.count; ++t) leaf(refs[k.first + t]);
         offset += k.count;
       }
     }
-    out.nodes.resize(out.nodes.size() + (size_t)inner * W8_NODE_WORDS, 0);
-    w = &out.nodes[(size_t)task.wide * W8_NODE_WORDS];
+    nodes.resize(nodes.size() + (size_t)inner * W8_NODE_WORDS, 0);
+    uint32_t* w = &nodes[(size_t)task.wide * W8_NODE_WORDS];
     for (int a = 0; a < 3; ++a) w[a] = as_bits(p[a]);
     w[3] = (uint32_t)(ex[0] + 127) | (uint32_t)(ex[1] + 127) << 8 | (uint32_t)(ex[2] + 127) << 16 | imask << 24;
     w[4] = child_base;
-    w[5] = tri_base;
+    w[5] = leaf_base;
     w[6] = meta[0] | meta[1] << 8 | meta[2] << 16 | (uint32_t)meta[3] << 24;
     w[7] = meta[4] | meta[5] << 8 | meta[6] << 16 | (uint32_t)meta[7] << 24;
     for (int plane = 0; plane < 6; ++plane) {
@@ -327,6 +324,43 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
     for (int s = 0; s < 8; ++s)
       if (slot_of[s] >= 0 && bn[kids[slot_of[s]]].count == 0) queue.push_back({next++, kids[slot_of[s]], task.level + 1});
   }
+}
+
+}  // namespace
+
+void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
+  out = Wide8Blas{};
+  if (tris.empty()) return;
+  Binary bin(tris);
+  const int broot = bin.build();
+  std::vector<BNode> bn = bin.nodes();
+  struct TriLeaf {
+    const std::vector<SrcTri>& tris;
+    std::vector<uint32_t>& words;
+    uint32_t base() const { return (uint32_t)(words.size() / W8_TRI_WORDS); }
+    void operator()(uint32_t ref) {
+      const SrcTri& src = tris[ref];
+      for (int j = 0; j < 9; ++j) words.push_back(as_bits(src.v[j]));
+      words.push_back(src.ident);
+      words.push_back(src.ref);
+      words.push_back(0);
+    }
+  } leaf{tris, out.tris};
+  emit_wide8(bn, broot, bin.refs(), out.nodes, out.max_exponent, out.depth, leaf);
+}
+
+void build_wide8_top(const std::vector<Aabb>& boxes, Wide8Top& out) {
+  out = Wide8Top{};
+  if (boxes.empty()) return;
+  Binary bin(boxes);
+  const int broot = bin.build();
+  std::vector<BNode> bn = bin.nodes();
+  struct InstanceLeaf {
+    std::vector<uint32_t>& items;
+    uint32_t base() const { return (uint32_t)items.size(); }
+    void operator()(uint32_t ref) { items.push_back(ref); }
+  } leaf{out.items};
+  emit_wide8(bn, broot, bin.refs(), out.nodes, out.max_exponent, out.depth, leaf);
 }
 
 namespace {
@@ -461,6 +495,37 @@ bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8
     out.inst[2 * i + 1] = tri_base[blas_of[i]];
   }
   out.blas_count = nb;
+  build_wide8_top_of(layout, w, out.top_nodes, out.top_items, &out.top_depth);
+  return true;
+}
+
+bool build_wide8_top_of(uint32_t layout, const uint32_t* w, std::vector<uint32_t>& nodes, std::vector<uint32_t>& items,
+                        uint32_t* depth) {
+  nodes.clear(), items.clear();
+  const uint32_t count = w[0];
+  if (w[1] == 0 || count < 2) return false;  // a flat instance list: the walk loops over it
+  const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
+  std::vector<Aabb> boxes;
+  std::vector<uint32_t> which;
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint32_t* r = w + header + stride * (size_t)i;
+    Aabb b;
+    bool ok = true;
+    for (int a = 0; a < 3; ++a) {
+      b.lo[a] = as_float(r[12 + a]), b.hi[a] = as_float(r[15 + a]);
+      ok = ok && std::isfinite(b.lo[a]) && std::isfinite(b.hi[a]) && b.lo[a] <= b.hi[a];
+    }
+    if (ok) boxes.push_back(b), which.push_back(i);
+  }
+  if (boxes.empty()) return false;
+  Wide8Top top;
+  build_wide8_top(boxes, top);
+  // the walk's top stack holds a group entry a level plus one node's eight leaves
+  if (top.max_exponent > W8_MAX_EXPONENT || top.depth + 9 > W8_TOP_STACK) return false;
+  for (uint32_t& it : top.items) it = which[it];
+  nodes = std::move(top.nodes);
+  items = std::move(top.items);
+  if (depth) *depth = top.depth;
   return true;
 }
 

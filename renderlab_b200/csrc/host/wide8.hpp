@@ -53,6 +53,19 @@ struct Wide8Scene {
   std::vector<uint32_t> inst;  // 2 words per instance: node base, triangle base
   size_t blas_count = 0;
   uint32_t depth = 0;  // the deepest BLAS's levels
+  // the 8-wide top level (empty: the scene is a flat instance list, or keeps its BVH4 top level)
+  std::vector<uint32_t> top_nodes, top_items;
+  uint32_t top_depth = 0;
+};
+
+// An 8-wide top level over instance world boxes, in the BLAS node format: a leaf slot's `count`
+// items (one: W8_MAX_LEAF) are instance indices at items[node word 5 + offset]; node 0 is the root
+// and nodes are numbered breadth first, so the upper levels are the lowest node indices.
+struct Wide8Top {
+  std::vector<uint32_t> nodes;
+  std::vector<uint32_t> items;
+  int max_exponent = -126;
+  uint32_t depth = 0;
 };
 
 // Source triangle for the builder: f32 vertices plus identity words.
@@ -62,11 +75,26 @@ struct SrcTri {
 };
 
 void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out);
+struct Aabb;
+void build_wide8_top(const std::vector<Aabb>& boxes, Wide8Top& out);
+// Entries of the WIDE8 walk's top-level stack (pairs of words): a level's group, plus one node's
+// eight instance leaves.
+constexpr uint32_t W8_TOP_STACK = 32;
+// The 8-wide top level of a packed scene's instances (over the world boxes of its records, words
+// 12-17), when it has a top level; false (nothing built) for a flat instance list, or when the
+// instances span more than the node scale allows or the tree is too deep for the walk's stack:
+// the walk then uses the packed BVH4 top level.
+bool build_wide8_top_of(uint32_t layout, const uint32_t* words, std::vector<uint32_t>& nodes,
+                        std::vector<uint32_t>& items, uint32_t* depth = nullptr);
 bool build_wide8_scene(uint32_t layout, const uint32_t* words, size_t n_words, Wide8Scene& out, std::string& err,
                        int threads);
 // Checks a built layout (wide8_check.cpp): ranges, one leaf per triangle, every child box
 // enclosing its child in exact arithmetic, inverted empty slots, the recorded depth. info: nodes,
 // triangles, depth, distinct BLAS.
 bool check_wide8_scene(const Wide8Scene& s, uint32_t info[4], std::string& err);
+// Checks the 8-wide top level of a scene built from `words`: every instance with a usable world
+// box in exactly one leaf, every child box enclosing the world boxes below it, nodes after their
+// parents, the recorded depth within the walk's stack.
+bool check_wide8_top(uint32_t layout, const uint32_t* words, const Wide8Scene& s, std::string& err);
 
 }  // namespace rtb

@@ -92,7 +92,78 @@ bool check_node(const Wide8Scene& s, uint32_t node, uint32_t level, std::vector<
   return true;
 }
 
+// The same for a node of the 8-wide top level: its leaves hold instance indices, and a child box
+// must enclose the world boxes (record words 12-17) of the instances below it.
+bool check_top_node(const Wide8Scene& s, const uint32_t* words, size_t header, size_t stride, uint32_t count,
+                    uint32_t node, uint32_t level, std::vector<uint8_t>& seen_node, std::vector<uint8_t>& seen_inst,
+                    uint32_t& depth, Extent& ext, std::string& err) {
+  const size_t nn = s.top_nodes.size() / W8_NODE_WORDS;
+  if (node >= nn) return err = "top-level node index out of range", false;
+  if (seen_node[node]) return err = "a top-level node is reached twice", false;
+  seen_node[node] = 1;
+  depth = std::max(depth, level);
+  const uint32_t* w = &s.top_nodes[(size_t)node * W8_NODE_WORDS];
+  double p[3], scale[3];
+  for (int a = 0; a < 3; ++a) {
+    const int e = (int)((w[3] >> (8 * a)) & 255u) - 127;
+    if (e > W8_MAX_EXPONENT || e < -126) return err = "top-level node scale exponent out of range", false;
+    p[a] = as_float(w[a]);
+    scale[a] = std::ldexp(1.0, e);
+  }
+  const uint32_t imask = w[3] >> 24, child_base = w[4], item_base = w[5];
+  for (int slot = 0; slot < 8; ++slot) {
+    const uint32_t meta = ((slot < 4 ? w[6] : w[7]) >> (8 * (slot & 3))) & 255u;
+    const bool inner = (imask >> slot) & 1u;
+    double lo[3], hi[3];
+    for (int a = 0; a < 3; ++a) lo[a] = p[a] + byte_of(w, a, slot) * scale[a], hi[a] = p[a] + byte_of(w, 3 + a, slot) * scale[a];
+    if (!inner && meta == 0) continue;
+    Extent child;
+    if (inner) {
+      const uint32_t c = child_base + (uint32_t)__builtin_popcount(imask & ((1u << slot) - 1u));
+      if (c <= node) return err = "top-level child not after its parent", false;
+      if (!check_top_node(s, words, header, stride, count, c, level + 1, seen_node, seen_inst, depth, child, err)) return false;
+    } else {
+      for (uint32_t k = 0; k < (meta >> 5); ++k) {
+        const size_t at = (size_t)item_base + (meta & 31u) + k;
+        if (at >= s.top_items.size()) return err = "top-level item out of range", false;
+        const uint32_t i = s.top_items[at];
+        if (i >= count) return err = "top-level leaf names no instance", false;
+        if (seen_inst[i]++) return err = "an instance is in two top-level leaves", false;
+        const uint32_t* r = words + header + stride * (size_t)i;
+        double l[3], h[3];
+        for (int a = 0; a < 3; ++a) l[a] = as_float(r[12 + a]), h[a] = as_float(r[15 + a]);
+        child.grow(l, h);
+      }
+    }
+    if (!child.within(lo, hi)) return err = "a top-level child box does not enclose its instances' world boxes", false;
+    ext.grow(child.lo, child.hi);
+  }
+  return true;
+}
+
 }  // namespace
+
+bool check_wide8_top(uint32_t layout, const uint32_t* words, const Wide8Scene& s, std::string& err) {
+  if (s.top_nodes.empty()) return true;  // no 8-wide top level: the walk uses the packed one
+  const uint32_t count = words[0];
+  const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
+  std::vector<uint8_t> seen_node(s.top_nodes.size() / W8_NODE_WORDS, 0), seen_inst(count, 0);
+  uint32_t depth = 0;
+  Extent ext;
+  if (!check_top_node(s, words, header, stride, count, 0, 1, seen_node, seen_inst, depth, ext, err)) return false;
+  if (std::find(seen_node.begin(), seen_node.end(), 0) != seen_node.end()) return err = "an unreachable top-level node", false;
+  for (uint32_t i = 0; i < count; ++i) {
+    const uint32_t* r = words + header + stride * (size_t)i;
+    bool valid = true;
+    for (int a = 0; a < 3; ++a) {
+      const float l = as_float(r[12 + a]), h = as_float(r[15 + a]);
+      valid = valid && std::isfinite(l) && std::isfinite(h) && l <= h;
+    }
+    if (valid && !seen_inst[i]) return err = "an instance no top-level leaf holds", false;
+  }
+  if (depth != s.top_depth || depth + 9 > W8_TOP_STACK) return err = "top-level depth differs from the record or the walk's stack", false;
+  return true;
+}
 
 bool check_wide8_scene(const Wide8Scene& s, uint32_t info[4], std::string& err) {
   const size_t nn = s.nodes.size() / W8_NODE_WORDS, nt = s.tris.size() / W8_TRI_WORDS;

@@ -55,7 +55,19 @@ struct W8View {
   const uint4* nodes;     // 5 uint4 a node
   const uint4* tris;      // 3 uint4 a triangle
   const uint32_t* inst;   // 2 words an instance: node base, triangle base
+  // the 8-wide top level (null: walk the packed BVH4 top level), breadth first from its root, and
+  // its leaves' instance indices
+  const uint4* top = nullptr;
+  const uint32_t* top_items = nullptr;
+  uint32_t top_count = 0;
 };
+
+// Top-level nodes staged in shared memory by every block of the per-ray walk (the first levels,
+// which every ray reads): 64 nodes, 5 KB.
+constexpr uint32_t W8_TOP_CACHE = 64;
+// Pairs of words in the per-ray walk's 8-wide top-level stack: a group entry (first child node,
+// pending bits | inner mask << 8) a level, and one node's leaf instances (instance, 0).
+constexpr uint32_t W8_TOP_STACK = 32;
 
 struct W8Best {
   float t;          // f32 t of the best candidate (f32(t64) once re-tested)
@@ -613,6 +625,51 @@ __global__ void __launch_bounds__(256) k_wide8_final(const uint32_t* __restrict_
   w8_final_hit<LAYOUT>(w, V, load_ray(e.rays, i), o);
 }
 
+RT_DEV uint32_t octant_of(const F3& d) {
+  return (d.x < 0.0f ? 1u : 0u) | (d.y < 0.0f ? 2u : 0u) | (d.z < 0.0f ? 4u : 0u);
+}
+
+// One node of the 8-wide top level (world space): its children's quantised boxes against the
+// world ray and the lane's bound. The inner children met become one group entry; each leaf met
+// pushes its instance above it, the first in visiting order on top, so a node's instances are
+// entered before the walk goes deeper.
+template <bool COUNT>
+RT_DEV void w8_top_node(const W8View& V, const uint4* cache, uint32_t cached, uint32_t node, const W8Lane& L,
+                        uint32_t* tstack, uint32_t& tsp, DevStatus* st, unsigned long long* cnt) {
+  w8_count<COUNT>(cnt, W8C_TOP_NODES);
+  uint4 a0, a1, a2, a3, a4;
+  if (node < cached) {
+    const uint4* np = cache + 5 * node;
+    a0 = np[0], a1 = np[1], a2 = np[2], a3 = np[3], a4 = np[4];
+  } else {
+    const uint4* np = V.top + 5 * (size_t)node;
+    a0 = __ldg(np), a1 = __ldg(np + 1), a2 = __ldg(np + 2), a3 = __ldg(np + 3), a4 = __ldg(np + 4);
+  }
+  W8Ray TW;
+  TW.o = L.ray.o;
+  TW.inv = L.world_inv;
+  TW.oct = octant_of(L.ray.d);
+  const W8Best& b = L.best;
+  const float lim = b.hit ? b.t + 2.0f * b.band + 2.0f * W8_TIE * b.t : L.ray.tmax;
+  const uint32_t hits = w8_box_hits(TW, a0, a2, a3, a4, L.ray.tmin, lim);
+  const uint32_t imask = a0.w >> 24;
+  const uint32_t inner = oct_permute(hits & imask, TW.oct);
+  if (inner) {
+    if (tsp + 2 <= 2 * W8_TOP_STACK) tstack[tsp] = a1.x, tstack[tsp + 1] = inner | imask << 8, tsp += 2;
+    else atomicAdd(&st->stack_drops, 1ull);
+  }
+  for (uint32_t leaves = oct_permute(hits & ~imask, TW.oct); leaves;) {
+    const uint32_t k = 31 - __clz(leaves);
+    leaves &= ~(1u << k);
+    const uint32_t s = k ^ TW.oct;
+    const uint32_t m = ((s < 4 ? a1.z : a1.w) >> (8 * (s & 3))) & 0xffu;
+    for (uint32_t j = m >> 5; j-- > 0;) {  // an empty slot met all the same has no items
+      if (tsp + 2 <= 2 * W8_TOP_STACK) tstack[tsp] = __ldg(V.top_items + a1.y + (m & 31u) + j), tstack[tsp + 1] = 0, tsp += 2;
+      else atomicAdd(&st->stack_drops, 1ull);
+    }
+  }
+}
+
 // Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
 // step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
 // re-converges at the top of the loop.
@@ -625,11 +682,18 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
     __shared__ uint2 columns[SS * BLOCK];
     stack.col = columns + threadIdx.x;
   }
-  uint32_t tstack[STACK];
+  // the packed BVH4 top level's stack (STACK items), or the 8-wide top level's (word pairs)
+  uint32_t tstack[STACK > 2 * W8_TOP_STACK ? STACK : 2 * W8_TOP_STACK];
   W8Lane L;
   L.phase = 0;
   const uint32_t count = ld(w, 0), top = ld(w, 1), root = ld(w, 2);
   const size_t top_base = LAYOUT == 0 ? top : (top & ~3u);
+  // the 8-wide top level's first nodes, staged once per block
+  __shared__ uint4 top_cache[5 * W8_TOP_CACHE];
+  const bool top8 = top != 0 && V.top != nullptr;
+  const uint32_t cached = top8 ? min(V.top_count, W8_TOP_CACHE) : 0u;
+  for (uint32_t i = threadIdx.x; i < 5 * cached; i += BLOCK) top_cache[i] = __ldg(V.top + i);
+  __syncthreads();
   bool drained = false;
   for (;;) {
     __syncwarp();
@@ -656,7 +720,11 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       L.phase = 1;
       L.flat = 0;
       L.tsp = 0;
-      if (top != 0 && count != 0) tstack[L.tsp++] = root;
+      if (top8) {  // the root as a group of one: slot 0 of an all-inner group at node 0
+        tstack[0] = 0, tstack[1] = (1u << octant_of(L.ray.d)) | 0xffu << 8, L.tsp = 2;
+      } else if (top != 0 && count != 0) {
+        tstack[L.tsp++] = root;
+      }
     }
     if (!__any_sync(0xffffffffu, L.phase != 0)) {
       if (drained) break;
@@ -681,6 +749,21 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       }
       if (L.tsp == 0) {
         w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
+        continue;
+      }
+      if (top8) {
+        L.tsp -= 2;
+        const uint32_t ex = tstack[L.tsp], ey = tstack[L.tsp + 1];
+        if (ey == 0) {  // an instance leaf
+          w8_enter<LAYOUT, AM, COUNT>(w, V, L, ex, cnt, true);
+          continue;
+        }
+        uint32_t bits = ey & 0xffu;  // a group: its first pending child now, the rest back on the stack
+        const uint32_t imask = ey >> 8, k = __ffs(bits) - 1;
+        bits &= bits - 1;
+        if (bits) tstack[L.tsp] = ex, tstack[L.tsp + 1] = bits | imask << 8, L.tsp += 2;
+        const uint32_t slot = k ^ octant_of(L.ray.d);
+        w8_top_node<COUNT>(V, top_cache, cached, ex + __popc(imask & ((1u << slot) - 1u)), L, tstack, L.tsp, st, cnt);
         continue;
       }
       const uint32_t item = tstack[--L.tsp];

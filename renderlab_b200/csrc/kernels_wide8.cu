@@ -76,6 +76,11 @@ bool view_of(const SceneView& s, rtk::W8View& v) {
   v.nodes = reinterpret_cast<const uint4*>(base + s.w8_nodes_at);
   v.tris = reinterpret_cast<const uint4*>(base + s.w8_tris_at);
   v.inst = base + s.w8_inst_at;
+  if (s.w8_top) {
+    v.top = static_cast<const uint4*>(s.w8_top);
+    v.top_items = static_cast<const uint32_t*>(s.w8_top) + s.w8_top_items_at;
+    v.top_count = s.w8_top_nodes;
+  }
   return true;
 }
 

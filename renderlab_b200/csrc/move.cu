@@ -195,6 +195,7 @@ extern "C" rt_status rt_scene_move_instances(rt_ctx* ctx, rt_scene* scene, const
     if (rtb::is_singular(placed[i])) return fail(ctx, RT_ERR_LAYOUT, "instance %u: singular placement", i);
   }
   if (n == 0) return RT_OK;
+  scene->w8_top_valid = false;  // the instances move: the packed top level until re-prepared
   const size_t need = sizeof(Moved) * n + 24 * (size_t)n_meshes;
   if (need > scene->move_bytes) {
     RT_CUDA(ctx, cudaFree(scene->d_move));

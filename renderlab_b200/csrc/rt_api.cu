@@ -73,6 +73,51 @@ rt_status check_trace_args(rt_ctx* ctx, const rt_scene* scene, rt_mode mode, rt_
 
 }  // namespace
 
+namespace {
+
+// Replaces the scene's 8-wide top level with these nodes and items (none: the walk uses the
+// packed top level).
+rt_status upload_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& nodes, const std::vector<uint32_t>& items) {
+  if (scene->d_w8_top) {
+    cudaFree(scene->d_w8_top);
+    scene->device_bytes -= scene->w8_top_bytes;
+    ctx->scene_bytes -= scene->w8_top_bytes;
+    scene->d_w8_top = nullptr, scene->w8_top_bytes = 0, scene->w8_top_nodes = 0;
+  }
+  scene->w8_top_valid = false;
+  if (nodes.empty()) return RT_OK;
+  const size_t items_at = nodes.size(), total = items_at + std::max<size_t>(items.size(), 1);
+  void* d = nullptr;
+  if (cudaMalloc(&d, total * 4) != cudaSuccess) {
+    cudaGetLastError();
+    return fail(ctx, RT_ERR_OOM, "device allocation of %zu bytes for the 8-wide top level failed", total * 4);
+  }
+  cudaError_t e = cudaMemcpy(d, nodes.data(), nodes.size() * 4, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess && !items.empty())
+    e = cudaMemcpy(static_cast<uint32_t*>(d) + items_at, items.data(), items.size() * 4, cudaMemcpyHostToDevice);
+  if (e != cudaSuccess) {
+    cudaFree(d);
+    return fail(ctx, RT_ERR_CUDA, "8-wide top-level upload: %s", cudaGetErrorString(e));
+  }
+  scene->d_w8_top = d;
+  scene->w8_top_bytes = total * 4;
+  scene->w8_top_items_at = items_at;
+  scene->w8_top_nodes = (uint32_t)(nodes.size() / rtb::W8_NODE_WORDS);
+  scene->w8_top_valid = true;
+  scene->device_bytes += scene->w8_top_bytes;
+  ctx->scene_bytes += scene->w8_top_bytes;
+  return RT_OK;
+}
+
+// Rebuilds only the 8-wide top level, from the scene's current records.
+rt_status prepare_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& words) {
+  std::vector<uint32_t> nodes, items;
+  rtb::build_wide8_top_of(scene->layout, words.data(), nodes, items);
+  return upload_top(ctx, scene, nodes, items);
+}
+
+}  // namespace
+
 extern "C" {
 
 uint32_t rt_abi_version(void) { return RT_ABI_VERSION; }
@@ -211,6 +256,7 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
     return fail(ctx, RT_ERR_LAYOUT, "records rejected: %s", err.c_str());
   RT_CUDA(ctx, cudaMemcpy(scene->d_words, words, n_words * 4, cudaMemcpyHostToDevice));
   scene->info = info;
+  scene->w8_top_valid = false;  // the instances' boxes may have moved: the packed top level until re-prepared
   return RT_OK;
 }
 
@@ -219,10 +265,11 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   if (kernel != RT_KERNEL_WIDE8 && kernel != RT_KERNEL_WIDE8_PACKET) return RT_OK;  // PLAIN, FAST: the packed words
   if (scene->layout == RT_LAYOUT_REFLECTION_BVH2)
     return fail(ctx, RT_ERR_UNSUPPORTED, "the legacy BVH2 layout is traced by the PLAIN kernel");
-  if (scene->d_wide8) return RT_OK;
+  if (scene->d_wide8 && (scene->w8_top_valid || scene->info.top == 0)) return RT_OK;
   std::vector<uint32_t> words(scene->n_words);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));
   RT_CUDA(ctx, cudaMemcpy(words.data(), scene->d_words, scene->n_words * 4, cudaMemcpyDeviceToHost));
+  if (scene->d_wide8) return prepare_top(ctx, scene, words);  // the BLASes stand; the instances moved
   rtb::Wide8Scene w8;
   std::string err;
   const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
@@ -252,7 +299,7 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   scene->w8_depth = w8.depth;
   scene->device_bytes += scene->wide8_bytes;
   ctx->scene_bytes += scene->wide8_bytes;
-  return RT_OK;
+  return upload_top(ctx, scene, w8.top_nodes, w8.top_items);
 }
 
 rt_status rt_wide8_check(rt_layout layout, const uint32_t* words, size_t n_words, uint32_t info[4], char* err,
@@ -264,7 +311,7 @@ rt_status rt_wide8_check(rt_layout layout, const uint32_t* words, size_t n_words
   const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
   bool ok = rtb::validate_scene((uint32_t)layout, words, n_words, si, why) &&
             rtb::build_wide8_scene((uint32_t)layout, words, n_words, w8, why, threads) &&
-            rtb::check_wide8_scene(w8, info, why);
+            rtb::check_wide8_scene(w8, info, why) && rtb::check_wide8_top((uint32_t)layout, words, w8, why);
   if (!ok && err && err_len) std::snprintf(err, err_len, "%s", why.c_str());
   return ok ? RT_OK : RT_ERR_LAYOUT;
 }
@@ -281,6 +328,7 @@ rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene) {
   cudaSetDevice(ctx->device);
   cudaFree(scene->d_words);
   cudaFree(scene->d_wide8);
+  cudaFree(scene->d_w8_top);
   cudaFree(scene->d_move);
   cudaFree(scene->d_top_order);
   for (auto& kv : scene->refit) cudaFree(kv.second.d_order);

@@ -61,3 +61,18 @@ def test_the_check_rejects_what_the_upload_rejects():
     bad[0] = 1 << 20  # more instance records than words
     with pytest.raises(A.RtError, match="LAYOUT"):
         A.wide8_check(A.LAYOUT_REFLECTION, bad)
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_top_level_encloses_every_instance(layout):
+    """Scenes with a top level also get an 8-wide one over the instances' world boxes: the check
+    walks it from its root and requires every instance in exactly one leaf, every child box to
+    enclose the world boxes below it in exact arithmetic, and the depth the walk's stack allows --
+    for 900 cube instances and for rotated, scaled instances of several meshes."""
+    mesh, inst = S.cubes_instanced(30)
+    A.wide8_check(layout, A.pack_scene(layout, [A.Blas(mesh.positions, mesh.indices)], inst))
+    ms = S.multi_blas(n_blas=6, n_instances=2_000, tri_lo=500.0, tri_hi=4_000.0, config=9)
+    w = A.pack_scene(layout, [A.Blas(m.positions, m.indices) for m in ms.meshes], ms.instances)
+    assert w[1] != 0
+    info = A.wide8_check(layout, w)
+    assert info["blas"] == 6
