@@ -169,7 +169,15 @@ RT_DEV void w8_setup(W8Ray& R) {
 // The triangle test's part for instance `inst` of the packed words (record rows at `r`): the
 // shear of Woop, Benthin and Wald (2013) for the object-space direction, and the error of the
 // f32 object-space origin against the f64 reference's (ray64's arithmetic over the same rows).
-__device__ __noinline__ void w8_shear(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray& R) {
+#ifndef RT_W8_LAZY
+#define RT_W8_LAZY 0
+#endif
+#if RT_W8_LAZY == 2
+__device__ __noinline__
+#else
+__device__ __forceinline__
+#endif
+void w8_shear(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray& R) {
   const float ax = fabsf(R.d.x), ay = fabsf(R.d.y), az = fabsf(R.d.z);
   const int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
   int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
@@ -291,7 +299,9 @@ template <uint32_t LAYOUT, int AM, bool COUNT>
 RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, W8Ray& R, const Ray& ray, uint32_t inst,
                          uint32_t tri, W8Best& best, unsigned long long* cnt, bool lane_any) {
   w8_count<COUNT>(cnt, W8C_TRIS);
+#if RT_W8_LAZY > 0
   if (!R.sheared) w8_shear(w, (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * inst, ray.o, R);
+#endif
   const uint4 q0 = __ldg(V.tris + 3 * (size_t)tri), q1 = __ldg(V.tris + 3 * (size_t)tri + 1),
               q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
   const F3 v0 = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
@@ -490,6 +500,9 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   L.R.d = {dot3({r00, r01, r02}, L.ray.d), dot3({r10, r11, r12}, L.ray.d), dot3({r20, r21, r22}, L.ray.d)};
   w8_setup(L.R);
   if (!L.R.valid) return;
+#if RT_W8_LAZY == 0
+  w8_shear(w, r, L.ray.o, L.R);
+#endif
   L.inst = i;
   L.node = root;
   L.g_bits = 0;

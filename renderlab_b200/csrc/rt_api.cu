@@ -111,9 +111,11 @@ rt_status upload_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& 
 
 // Rebuilds only the 8-wide top level, from the scene's current records.
 rt_status prepare_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& words) {
-  std::vector<uint32_t> nodes, items;
-  rtb::build_wide8_top_of(scene->layout, words.data(), nodes, items);
-  return upload_top(ctx, scene, nodes, items);
+  rtb::Wide8Scene top;
+  std::string err;
+  rtb::build_wide8_top_of(scene->layout, words.data(), top.top_nodes, top.top_items, &top.top_depth);
+  if (!rtb::check_wide8_top(scene->layout, words.data(), top, err)) top.top_nodes.clear();  // the packed top level
+  return upload_top(ctx, scene, top.top_nodes, top.top_items);
 }
 
 }  // namespace
@@ -299,6 +301,7 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   scene->w8_depth = w8.depth;
   scene->device_bytes += scene->wide8_bytes;
   ctx->scene_bytes += scene->wide8_bytes;
+  if (!rtb::check_wide8_top(scene->layout, words.data(), w8, err)) w8.top_nodes.clear();  // the packed top level
   return upload_top(ctx, scene, w8.top_nodes, w8.top_items);
 }
 

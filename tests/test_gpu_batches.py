@@ -155,8 +155,8 @@ def test_tuner_plan_matches_plain(engine):
         dev = _device(batches)
         ch = T.tune(engine, scene, dev, refills=(8, 32), orders=("none", "octant"), reps=1)
         # plain 1, fast 2 x 2, wide8 2 x 2 with the local stack and 2 unsorted with the shared one
-        # (the cube BLAS is shallow); the packet walk is refused (the scene has a top level)
-        assert {t.kernel for t in ch.trials} == {"plain", "fast", "wide8"} and len(ch.trials) == 11
+        # (the cube BLAS is shallow), and the packet walk (over the top level too) with 2 orders
+        assert {t.kernel for t in ch.trials} == {"plain", "fast", "wide8", "wide8p"} and len(ch.trials) == 13
         assert {t.stack for t in ch.trials if t.kernel == "wide8"} == {"local", "shared"}
         ch.plan.launch()
         torch.cuda.synchronize()
