@@ -542,7 +542,8 @@ class Server:
     def submit(self, sid: int, rays, mode: int = CLOSEST, out=None) -> int:
         """rays: (n, 8) float32 host array (numpy, or a pinned torch CPU tensor). Returns a ticket."""
         n = len(rays)
-        words = hit_words(self.layouts[sid], mode)
+        # an unknown scene id goes to the library, which refuses it (RT_ERR_INVALID_ARG)
+        words = hit_words(self.layouts.get(sid, LAYOUT_REFLECTION), mode)
         if out is None:
             out = np.zeros((n, words) if words > 1 else (n,), np.uint32)
         rp = rays.data_ptr() if hasattr(rays, "data_ptr") else rays.ctypes.data

@@ -270,8 +270,16 @@ RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& dma
 // otherwise take registers from the walk). The candidate and, if the incumbent is still an f32
 // estimate, the incumbent are re-intersected with the f64 reference's arithmetic; the lower
 // (t, instance, triangle) wins. Returns true when the candidate is the new best.
+#ifndef RT_W8_RESOLVE_INLINE
+#define RT_W8_RESOLVE_INLINE 0
+#endif
 template <uint32_t LAYOUT>
-__device__ __noinline__ bool w8_resolve64(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t inst,
+#if RT_W8_RESOLVE_INLINE
+__device__ __forceinline__
+#else
+__device__ __noinline__
+#endif
+bool w8_resolve64(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t inst,
                                           uint32_t tri, uint32_t ident, uint32_t ref, W8Best& best) {
   double t64 = 0.0, u64 = 0.0, v64 = 0.0;
   if (!mt64<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) return false;
