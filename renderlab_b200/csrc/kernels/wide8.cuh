@@ -35,13 +35,15 @@ constexpr uint32_t W8_STACK = 32;
 // levels deep stacks at most W8_SSTACK - 1 groups).
 constexpr uint32_t W8_SSTACK = 16;
 // Resident 128-thread blocks per SM the register allocation is sized for: the per-ray walk
-// (RT_W8_MIN_BLOCKS) and the packet walk (RT_W8P_MIN_BLOCKS). The f64 paths and the lazy
-// instance setup are out of line, so the walks' hot loops fit these budgets.
+// (RT_W8_MIN_BLOCKS: 7, 72 registers) and the packet walk (RT_W8P_MIN_BLOCKS: 5, 96 registers).
+// The f64 resolution of uncertain candidates is out of line, so the hot loops fit these budgets
+// with a few bytes of spills. Measured on clusters-1M / clusters-4M GI rays against 4, 6 and 8
+// blocks: 7 is the fastest per-ray walk, 5 the fastest packet walk.
 #ifndef RT_W8_MIN_BLOCKS
-#define RT_W8_MIN_BLOCKS 4
+#define RT_W8_MIN_BLOCKS 7
 #endif
 #ifndef RT_W8P_MIN_BLOCKS
-#define RT_W8P_MIN_BLOCKS 4
+#define RT_W8P_MIN_BLOCKS 5
 #endif
 
 // Opt-in device counters of the WIDE8 walk (diagnostics and the bytes-per-ray roofline).
@@ -169,15 +171,7 @@ RT_DEV void w8_setup(W8Ray& R) {
 // The triangle test's part for instance `inst` of the packed words (record rows at `r`): the
 // shear of Woop, Benthin and Wald (2013) for the object-space direction, and the error of the
 // f32 object-space origin against the f64 reference's (ray64's arithmetic over the same rows).
-#ifndef RT_W8_LAZY
-#define RT_W8_LAZY 0
-#endif
-#if RT_W8_LAZY == 2
-__device__ __noinline__
-#else
-__device__ __forceinline__
-#endif
-void w8_shear(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray& R) {
+__device__ __forceinline__ void w8_shear(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray& R) {
   const float ax = fabsf(R.d.x), ay = fabsf(R.d.y), az = fabsf(R.d.z);
   const int kz = (ax >= ay && ax >= az) ? 0 : (ay >= az ? 1 : 2);
   int kx = kz == 2 ? 0 : kz + 1, ky = kx == 2 ? 0 : kx + 1;
@@ -210,6 +204,11 @@ void w8_shear(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray
                         fabs(o64(r + 8) - (double)R.o.z));
   R.oerr = e > 0.0 ? __double2float_ru(e) : 0.0f;
   R.sheared = true;
+}
+// The same, out of line: a lazy setup at an instance's first triangle (see W8Ray), which most
+// entries of an instance-heavy scene never reach, so its code stays out of the walk's registers.
+__device__ __noinline__ void w8_shear_late(const uint32_t* __restrict__ w, size_t r, const F3& world_o, W8Ray& R) {
+  w8_shear(w, r, world_o, R);
 }
 
 // Projected vertex (Ax, Ay, Az): one fixed chain of operations per vertex. `m` keeps the
@@ -270,16 +269,8 @@ RT_DEV int w8_triangle(const W8Ray& R, F3 v0, F3 v1, F3 v2, float& t, float& dma
 // otherwise take registers from the walk). The candidate and, if the incumbent is still an f32
 // estimate, the incumbent are re-intersected with the f64 reference's arithmetic; the lower
 // (t, instance, triangle) wins. Returns true when the candidate is the new best.
-#ifndef RT_W8_RESOLVE_INLINE
-#define RT_W8_RESOLVE_INLINE 0
-#endif
 template <uint32_t LAYOUT>
-#if RT_W8_RESOLVE_INLINE
-__device__ __forceinline__
-#else
-__device__ __noinline__
-#endif
-bool w8_resolve64(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t inst,
+__device__ __noinline__ bool w8_resolve64(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t inst,
                                           uint32_t tri, uint32_t ident, uint32_t ref, W8Best& best) {
   double t64 = 0.0, u64 = 0.0, v64 = 0.0;
   if (!mt64<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) return false;
@@ -303,13 +294,11 @@ bool w8_resolve64(const uint32_t* __restrict__ w, const W8View& V, const Ray& ra
 }
 
 // Considers one candidate triangle; returns true when an any-hit query is satisfied.
-template <uint32_t LAYOUT, int AM, bool COUNT>
+template <uint32_t LAYOUT, int AM, bool COUNT, bool LAZY = false>
 RT_DEV bool w8_candidate(const uint32_t* __restrict__ w, const W8View& V, W8Ray& R, const Ray& ray, uint32_t inst,
                          uint32_t tri, W8Best& best, unsigned long long* cnt, bool lane_any) {
   w8_count<COUNT>(cnt, W8C_TRIS);
-#if RT_W8_LAZY > 0
-  if (!R.sheared) w8_shear(w, (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * inst, ray.o, R);
-#endif
+  if (LAZY && !R.sheared) w8_shear_late(w, (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * inst, ray.o, R);
   const uint4 q0 = __ldg(V.tris + 3 * (size_t)tri), q1 = __ldg(V.tris + 3 * (size_t)tri + 1),
               q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
   const F3 v0 = {__uint_as_float(q0.x), __uint_as_float(q0.y), __uint_as_float(q0.z)};
@@ -431,7 +420,7 @@ struct W8GroupStack<0, BLOCK> {
   RT_DEV uint2& operator[](uint32_t i) { return e[i]; }
 };
 
-template <uint32_t LAYOUT, int AM, bool COUNT, class Stack>
+template <uint32_t LAYOUT, int AM, bool COUNT, bool LAZY, class Stack>
 RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, Stack& stack, DevStatus* st,
                     unsigned long long* cnt) {
   w8_count<COUNT>(cnt, W8C_NODES);
@@ -453,7 +442,7 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
     const uint32_t first = tri_base + (m & 31u), count = m >> 5;
     w8_count<COUNT>(cnt, W8C_LEAVES);
     for (uint32_t k = 0; k < count; ++k)
-      if (w8_candidate<LAYOUT, AM, COUNT>(w, V, R, L.ray, L.inst, first + k, L.best, cnt, L.any)) return true;
+      if (w8_candidate<LAYOUT, AM, COUNT, LAZY>(w, V, R, L.ray, L.inst, first + k, L.best, cnt, L.any)) return true;
   }
   const uint32_t inner = oct_permute(hits & imask, R.oct);
   if (inner) {
@@ -483,7 +472,7 @@ RT_DEV bool w8_next(W8Lane& L, Stack& stack) {
 }
 
 // Enters instance i when its world box survives; sets up the object-space ray.
-template <uint32_t LAYOUT, int AM, bool COUNT>
+template <uint32_t LAYOUT, int AM, bool COUNT, bool LAZY = false>
 // `from_top`: the instance comes from a top-level leaf, whose box the walk has just tested. That
 // box is the instance's world box, so its test here could only pass: the walk skips it (WIDE8's
 // results do not depend on which extra instances it enters, only its work does). A flat instance
@@ -508,9 +497,7 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   L.R.d = {dot3({r00, r01, r02}, L.ray.d), dot3({r10, r11, r12}, L.ray.d), dot3({r20, r21, r22}, L.ray.d)};
   w8_setup(L.R);
   if (!L.R.valid) return;
-#if RT_W8_LAZY == 0
-  w8_shear(w, r, L.ray.o, L.R);
-#endif
+  if (!LAZY) w8_shear(w, r, L.ray.o, L.R);
   L.inst = i;
   L.node = root;
   L.g_bits = 0;
@@ -694,7 +681,7 @@ RT_DEV void w8_top_node(const W8View& V, const uint4* cache, uint32_t cached, ui
 // Persistent warps, one ray per lane, refilled as rays end; every iteration a lane takes one
 // step (a top-level node, an instance entry, or one 8-wide node with its leaves) and the warp
 // re-converges at the top of the loop.
-template <uint32_t LAYOUT, int AM, int BLOCK, bool COUNT, class Src, int SS = 0>
+template <uint32_t LAYOUT, int AM, int BLOCK, bool COUNT, class Src, int SS = 0, bool LAZY = false>
 __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                  unsigned int* __restrict__ counter, uint32_t n, DevStatus* st,
                                                  unsigned long long* cnt, uint32_t refill) {
@@ -755,7 +742,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       if (L.node == EMPTY && !w8_next(L, stack)) {
         L.phase = 1;
       } else {
-        if (w8_node<LAYOUT, AM, COUNT>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
+        if (w8_node<LAYOUT, AM, COUNT, LAZY>(w, V, L, stack, st, cnt)) w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
         continue;
       }
     }
@@ -765,7 +752,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
           w8_finish<LAYOUT, AM, COUNT>(w, V, L, src, cnt);
           continue;
         }
-        w8_enter<LAYOUT, AM, COUNT>(w, V, L, L.flat++, cnt, false);
+        w8_enter<LAYOUT, AM, COUNT, LAZY>(w, V, L, L.flat++, cnt, false);
         continue;
       }
       if (L.tsp == 0) {
@@ -776,7 +763,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
         L.tsp -= 2;
         const uint32_t ex = tstack[L.tsp], ey = tstack[L.tsp + 1];
         if (ey == 0) {  // an instance leaf
-          w8_enter<LAYOUT, AM, COUNT>(w, V, L, ex, cnt, true);
+          w8_enter<LAYOUT, AM, COUNT, LAZY>(w, V, L, ex, cnt, true);
           continue;
         }
         uint32_t bits = ey & 0xffu;  // a group: its first pending child now, the rest back on the stack
@@ -789,7 +776,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       }
       const uint32_t item = tstack[--L.tsp];
       if (item & LEAF) {
-        w8_enter<LAYOUT, AM, COUNT>(w, V, L, item & ~LEAF, cnt, true);
+        w8_enter<LAYOUT, AM, COUNT, LAZY>(w, V, L, item & ~LEAF, cnt, true);
         continue;
       }
       const W8Best& b = L.best;

@@ -84,6 +84,22 @@ bool view_of(const SceneView& s, rtk::W8View& v) {
   return true;
 }
 
+// Scenes with a top level set up each entered instance's triangle test lazily (at its first
+// triangle: most entries of an instance-heavy scene end at the BLAS root's boxes); flat scenes,
+// whose rays enter one or a few instances, set it up on entry.
+template <bool COUNT, int SS, bool LAZY>
+cudaError_t launch_one(const SceneView& s, const rtk::W8View& v, uint32_t mode, const rtk::OneBatch& src, uint32_t n,
+                       unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream, unsigned long long* cnt,
+                       uint32_t refill) {
+  using rtk::OneBatch;
+  if (s.layout == 0) {
+    return mode == 0 ? run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch, SS, LAZY>, s.words, v, src, counter, n, st, stream, cnt, refill)
+                     : run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch, SS, LAZY>, s.words, v, src, counter, n, st, stream, cnt, refill);
+  }
+  return mode == 0 ? run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch, SS, LAZY>, s.words, v, src, counter, n, st, stream, cnt, refill)
+                   : run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch, SS, LAZY>, s.words, v, src, counter, n, st, stream, cnt, refill);
+}
+
 template <bool COUNT, int SS>
 cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, const uint32_t* order, void* hits,
                        uint32_t n, unsigned int* counter, rtk::DevStatus* st, cudaStream_t stream,
@@ -91,16 +107,9 @@ cudaError_t launch_any(const SceneView& s, uint32_t mode, const float4* rays, co
   if (n == 0) return cudaSuccess;
   rtk::W8View v;
   if (!view_of(s, v)) return cudaErrorInvalidValue;
-  using rtk::OneBatch;
-  const OneBatch src{rays, order, hits};
-  cudaError_t e;
-  if (s.layout == 0) {
-    e = mode == 0 ? run(rtk::k_wide8<0, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill)
-                  : run(rtk::k_wide8<0, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
-  } else {
-    e = mode == 0 ? run(rtk::k_wide8<1, 0, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill)
-                  : run(rtk::k_wide8<1, 1, W8_BLOCK, COUNT, OneBatch, SS>, s.words, v, src, counter, n, st, stream, cnt, refill);
-  }
+  const rtk::OneBatch src{rays, order, hits};
+  const cudaError_t e = s.top ? launch_one<COUNT, SS, true>(s, v, mode, src, n, counter, st, stream, cnt, refill)
+                              : launch_one<COUNT, SS, false>(s, v, mode, src, n, counter, st, stream, cnt, refill);
   return then_final(e, mode == 0, s, v, src, n, stream);
 }
 
@@ -127,8 +136,11 @@ cudaError_t launch_wide8_batches(const SceneView& s, const rtk::BatchEntry* tabl
   if (!view_of(s, v)) return cudaErrorInvalidValue;
   using rtk::ManyBatches;
   const ManyBatches src{table, entries, order};
-#define RT_W8B(L, AM, SS) \
-  run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches, SS>, s.words, v, src, counter, total, st, stream, nullptr, refill)
+#define RT_W8B(L, AM, SS)                                                                                         \
+  (s.top ? run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches, SS, true>, s.words, v, src, counter, total, st, stream, \
+               nullptr, refill)                                                                                       \
+         : run(rtk::k_wide8<L, AM, W8_BLOCK, false, ManyBatches, SS, false>, s.words, v, src, counter, total, st,       \
+               stream, nullptr, refill))
   cudaError_t e;
   if (stack == 0) {
     if (s.layout == 0) e = uniform_mode == 0 ? RT_W8B(0, 0, 0) : (uniform_mode == 1 ? RT_W8B(0, 1, 0) : RT_W8B(0, 2, 0));
@@ -156,10 +168,14 @@ cudaError_t launch_wide8_lights(const SceneView& s, const void* cells, uint32_t 
   using rtk::LightRays;
   const LightRays src{static_cast<const rtk::GiCell*>(cells), static_cast<const rtk::GiLight*>(lights), n_lights, per_cell,
                       words};
-  if (stack == 0) return run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, 0>, s.words, v, src, counter, items, st, stream, nullptr, refill);
-  if (!shared_stack_fits(s)) return cudaErrorInvalidValue;
-  return run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, (int)rtk::W8_SSTACK>, s.words, v, src, counter, items, st, stream,
-             nullptr, refill);
+  if (stack != 0 && !shared_stack_fits(s)) return cudaErrorInvalidValue;
+  constexpr int SS = (int)rtk::W8_SSTACK;
+  if (s.top) {
+    return stack == 0 ? run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, 0, true>, s.words, v, src, counter, items, st, stream, nullptr, refill)
+                      : run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, SS, true>, s.words, v, src, counter, items, st, stream, nullptr, refill);
+  }
+  return stack == 0 ? run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, 0, false>, s.words, v, src, counter, items, st, stream, nullptr, refill)
+                    : run(rtk::k_wide8<0, 1, W8_BLOCK, false, LightRays, SS, false>, s.words, v, src, counter, items, st, stream, nullptr, refill);
 }
 
 namespace {
