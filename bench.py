@@ -62,7 +62,9 @@ def parse(argv=None):
     ap.add_argument("--config", type=int, default=3, choices=[1, 2, 3, 4, 5])
     ap.add_argument("--rates", default="1000,2000,5000,10000,20000", help="--config 5: Poisson arrival rates (req/s)")
     ap.add_argument("--requests", type=int, default=48, help="--config 5: requests per rate")
-    ap.add_argument("--kernel", default="auto", help="auto: the autotuner's choice; or plain / fast / wide8")
+    ap.add_argument("--kernel", default="auto",
+                    help="auto: the autotuner's choice; or plain / fast / wide8 / wide8p for every launch group, or "
+                         "one of them a group, comma-separated")
     ap.add_argument("--refill", type=int, default=0, help="with --kernel fast/wide8: the wavefront width")
     ap.add_argument("--order", default="none", help="with --kernel fast/wide8: the sort key")
     ap.add_argument("--stack", default="", help="with --kernel wide8: local or shared node-group stack")
@@ -699,7 +701,14 @@ def run_ours(args):
     engine = A.Engine(local)
     wl, scene = workload(args.config, engine, args.small)
     t_prep = time.perf_counter()
-    if args.kernel in ("auto", "wide8", "wide8p"):
+    # --kernel: "auto" (the autotuner), one kernel for every launch group, or one a group
+    # ("wide8p,wide8,wide8": how a profiling capture pins the plans the tuner chose)
+    forced = args.kernel.split(",") if args.kernel != "auto" else []
+    if forced and len(forced) == 1:
+        forced = forced * len(wl.groups)
+    if forced and len(forced) != len(wl.groups):
+        raise SystemExit(f"--kernel names {len(forced)} kernels for {len(wl.groups)} launch groups")
+    if args.kernel == "auto" or any(k in ("wide8", "wide8p") for k in forced):
         scene.prepare("wide8")  # derived layouts (the 8-wide BVH) are scene-upload work, untimed
     t_prep = time.perf_counter() - t_prep
     dev = [torch.from_numpy(b.rays).cuda() for b in wl.batches]
@@ -715,7 +724,7 @@ def run_ours(args):
     # ---- product plans: one per group, from the autotuner (or the forced kernel)
     t_tune = time.perf_counter()
     plans, tables = [], []
-    for g in wl.groups:
+    for gk, g in enumerate(wl.groups):
         batches = [(dev[i], wl.batches[i].mode) for i in g]
         if args.kernel == "auto":
             heavy = len(g) > 8  # the many-batch launch runs for seconds: one timed launch a candidate,
@@ -724,11 +733,11 @@ def run_ours(args):
                         kernels=("plain", "fast", "wide8") if heavy else T.KERNELS)
             plans.append(ch.plan)
             tables.append(ch.table()[:6])
-        elif args.kernel == "plain":
+        elif forced[gk] == "plain":
             plans.append(None)
         else:
-            plans.append(engine.plan(scene, batches, args.kernel, refill=args.refill, order=args.order,
-                                     stack=args.stack if args.kernel == "wide8" else ""))
+            plans.append(engine.plan(scene, batches, forced[gk], refill=args.refill, order=args.order,
+                                     stack=args.stack if forced[gk] == "wide8" else ""))
     t_tune = time.perf_counter() - t_tune
 
     def plain_step():
