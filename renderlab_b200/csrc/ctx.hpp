@@ -109,12 +109,12 @@ rt_status tlas_build_device(rt_ctx* ctx, const uint32_t* d_box_words, size_t str
 
 constexpr size_t GI_HIT_BYTES = 40, RS_HIT_BYTES = 20, ANY_HIT_BYTES = 4, RAY_BYTES = 32;
 #ifndef RT_HOST_CHUNK_LOG2
-#define RT_HOST_CHUNK_LOG2 19
+#define RT_HOST_CHUNK_LOG2 20
 #endif
 // Rays a host-buffer call stages per chunk (copies of one chunk overlap the next chunk's kernel).
-// 2^19: measured end to end on the clusters-1M step with four stages at 804 Mrays/s, against 790
-// for 2^20 (a longer first copy and last read-back) and 777 for 2^18 (775 with eight stages: each
-// launch's tail of idle lanes weighs more).
+// 2^20: measured end to end on the precision-4M step (16.8M rays, four stages) at 771 Mrays/s,
+// against 752 for 2^19 (more launches, each with its tail of idle lanes and its final pass) and
+// 773 for 2^21 (eight stages of 2^20: 776).
 constexpr uint32_t HOST_CHUNK = 1u << RT_HOST_CHUNK_LOG2;
 constexpr uint32_t COUNTER_SLOTS = 4096;
 
