@@ -284,12 +284,13 @@ def wide8_bytes(counters, layout, hit_bytes):
         + 48 * c["triangles"]
 
 
-# DRAM bytes per ray (read + write) that ncu measured on a launch, by (config, --small, kernel);
-# the capture command and figures are in profiles/k_wide8_clusters250k_gi.md. The capture is the
-# reduced clusters case (250k triangles, 1M GI rays); the full case reuses its bytes per ray,
-# since a ray's compulsory traffic is its own ray and hit plus its share of one scene read
-# (about 17 bytes a ray in both).
-TRAFFIC = {(2, True, "k_wide8"): 67.8, (2, False, "k_wide8"): 67.8}
+# DRAM bytes per ray (read + write) that ncu measured on the dominant launch -- the GI batch's
+# k_wide8 -- by (config, --small, kernel). Captured with
+#   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
+#       -k regex:^k_wide8$ -s 1 -c 1 python bench.py [--small] --steps 1 --warmup 3 --no-cpu --precision 0 --kernel wide8
+# (one pass; the launch is the first warm-up step's GI batch): precision-4M 1.05 GB read + 495.4 MB
+# written for 5,033,164 rays; the 1M-triangle reduced case 234.5 + 103.0 MB for 1,258,291 rays.
+TRAFFIC = {(3, False, "k_wide8"): (1.05e9 + 495.41e6) / 5_033_164, (3, True, "k_wide8"): (234.53e6 + 102.95e6) / 1_258_291}
 
 
 def hit_bytes(layout, mode):
@@ -614,6 +615,13 @@ def run_serving(args):
     rates = [float(x) for x in args.rates.split(",")]
     per_rate = []
     total_rays, total_s = 0, 0.0
+    bus = None
+    try:
+        bus = torch.cuda.get_device_properties(0).pci_bus_id
+    except AttributeError:
+        pass
+    clocks = Clocks()
+    clocks.start()
     for rate in rates:
         n_req = args.requests
         gaps = -np.log(1.0 - rng.uniform(n_req)) / rate
@@ -667,6 +675,7 @@ def run_serving(args):
                                         p99_ms=float(np.percentile(lat, 99)), max_ms=float(np.max(lat)))))
         total_rays += rays
         total_s += wall
+    clk = clocks.stop(bus)
     dev_bytes = srv.stats()["device_bytes"]
     srv.close()
     for sc in plain_scenes:
@@ -682,7 +691,7 @@ def run_serving(args):
                             config=5, kernel=kernel, launch_rays=1 << 22, slots=4),
                 latency_ms=dict(p50=top["p50_ms"], p99=top["p99_ms"], plain_p50=top["plain"]["p50_ms"],
                                 plain_p99=top["plain"]["p99_ms"]),
-                rates=per_rate,
+                rates=per_rate, clocks=clk,
                 e2e=dict(value=total_rays / total_s / 1e6, unit=UNIT, h2d_bytes_per_step=None, d2h_bytes_per_step=None,
                          path="rt_server_submit / rt_server_wait, pinned host buffers; timed from each rate's first "
                               "arrival to its last completion"),

@@ -45,9 +45,6 @@ constexpr uint32_t W8_SSTACK = 16;
 #ifndef RT_W8P_MIN_BLOCKS
 #define RT_W8P_MIN_BLOCKS 5
 #endif
-#ifndef RT_W8_NEAREST_FIRST
-#define RT_W8_NEAREST_FIRST 0
-#endif
 
 // Opt-in device counters of the WIDE8 walk (diagnostics and the bytes-per-ray roofline).
 enum W8Count { W8C_RAYS, W8C_TOP_NODES, W8C_INSTANCE_TESTS, W8C_NODES, W8C_LEAVES, W8C_TRIS, W8C_RETESTS, W8C_FINAL64, W8C_N };
@@ -363,10 +360,8 @@ struct W8Lane {
 
 // The eight child-box tests of one node for one ray: bit s is set when slot s's box meets
 // [tmin, lim] (conservatively: no box the ray meets is missed).
-// `near_slot` (when not null) receives the inner slot (a set bit of `imask`) whose box the ray
-// enters first, 8 when it meets none.
 RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, const uint4& a3, const uint4& a4, float tmin,
-                            float lim, uint32_t imask = 0, uint32_t* near_slot = nullptr) {
+                            float lim) {
   const float px = __uint_as_float(a0.x), py = __uint_as_float(a0.y), pz = __uint_as_float(a0.z);
   // A' = 2^(e+15) / d and C = (p - o) / d - A' per axis, so that a plane's t = q 2^e / d + (p - o) / d
   // is one fma of the decoded 1 + q 2^-15: fma(Q, A', C). The same rounded A' enters both terms,
@@ -394,8 +389,7 @@ RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, co
   const uint32_t fy0 = R.oct & 2u ? a2.z : a4.x, fy1 = R.oct & 2u ? a2.w : a4.y;
   const uint32_t nz0 = R.oct & 4u ? a4.z : a3.x, nz1 = R.oct & 4u ? a4.w : a3.y;
   const uint32_t fz0 = R.oct & 4u ? a3.x : a4.z, fz1 = R.oct & 4u ? a3.y : a4.w;
-  uint32_t hits = 0, best_s = 8;
-  float best_tn = INFINITY;
+  uint32_t hits = 0;
 #pragma unroll
   for (int s = 0; s < 8; ++s) {
     const uint32_t b = s & 3;
@@ -403,12 +397,8 @@ RT_DEV uint32_t w8_box_hits(const W8Ray& R, const uint4& a0, const uint4& a2, co
     const float tny = fmaf(q15(s < 4 ? ny0 : ny1, b), Ay, Bny), tfy = fmaf(q15(s < 4 ? fy0 : fy1, b), Ay, Bfy);
     const float tnz = fmaf(q15(s < 4 ? nz0 : nz1, b), Az, Bnz), tfz = fmaf(q15(s < 4 ? fz0 : fz1, b), Az, Bfz);
     const float tn = fmaxf(fmaxf(tnx, tny), fmaxf(tnz, tmin)), tf = fminf(fminf(tfx, tfy), fminf(tfz, lim));
-    if (tn <= tf) {
-      hits |= 1u << s;
-      if (near_slot && (imask >> s & 1u) && tn < best_tn) best_tn = tn, best_s = s;
-    }
+    if (tn <= tf) hits |= 1u << s;
   }
-  if (near_slot) *near_slot = best_s;
   return hits;
 }
 
@@ -441,12 +431,7 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const uint32_t child_base = a1.x, tri_base = a1.y, meta_lo = a1.z, meta_hi = a1.w;
   const W8Best& best = L.best;
   const float lim = best.hit ? best.t + 2.0f * best.band + W8_TIE * best.t : L.ray.tmax;
-#if RT_W8_NEAREST_FIRST
-  uint32_t near_slot;
-  const uint32_t hits = w8_box_hits(R, a0, a2, a3, a4, L.ray.tmin, lim, imask, &near_slot);
-#else
   const uint32_t hits = w8_box_hits(R, a0, a2, a3, a4, L.ray.tmin, lim);
-#endif
   // Empty slots hold inverted boxes, which no ray meets; one that is met all the same (a node
   // tiny beside its distance, where the widening exceeds 255 steps) has a zero count.
   uint32_t leaf_hits = hits & ~imask;
@@ -460,23 +445,6 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
       if (w8_candidate<LAYOUT, AM, COUNT, LAZY>(w, V, R, L.ray, L.inst, first + k, L.best, cnt, L.any)) return true;
   }
   const uint32_t inner = oct_permute(hits & imask, R.oct);
-#if RT_W8_NEAREST_FIRST
-  // The inner child the ray enters first is the next node; the others wait as a group, visited
-  // in octant order (WIDE8's results do not depend on the order; its work does).
-  L.node = EMPTY;
-  if (inner) {
-    const uint32_t rest = inner & ~(1u << (near_slot ^ R.oct));
-    if (rest) {
-      if (L.g_bits) {
-        if (L.sp < Stack::cap) stack[L.sp++] = make_uint2(L.g_base, L.g_bits | L.g_imask << 8);
-        else atomicAdd(&st->stack_drops, 1ull);
-      }
-      L.g_base = child_base, L.g_bits = rest, L.g_imask = imask;
-    }
-    L.node = child_base + __popc(imask & ((1u << near_slot) - 1u));
-  }
-  return false;
-#else
   if (inner) {
     if (L.g_bits) {
       if (L.sp < Stack::cap) stack[L.sp++] = make_uint2(L.g_base, L.g_bits | L.g_imask << 8);
@@ -486,7 +454,6 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   }
   L.node = EMPTY;
   return false;
-#endif
 }
 
 // The next node of the current group (or of a popped one); false when the BLAS is done.
