@@ -2,7 +2,9 @@
 move's (rt_move_instances_host), bit for bit, over moves in a row (the top level refit each time,
 header word 3 counting), across the rebuild after 64 refits (made on the device) and over the
 refits after it (in the rebuilt tree's level order); traced rays see the moved scene as the
-oracle does; and the 8-wide walk, derived before the moves, finds the same triangles after them."""
+oracle does; and the 8-wide walk, derived before the moves, finds the same triangles after them,
+through the packed top level while its own 8-wide top level is stale and through the rebuilt one
+after a new prepare."""
 import numpy as np
 import pytest
 
@@ -49,5 +51,10 @@ def test_device_move_equals_the_host_move(engine, layout):
         ids = slice(1, 5) if layout == A.LAYOUT_GI else slice(1, 3)
         same = (w8.reshape(want.shape)[:, ids] == want[:, ids]).all(axis=1)
         assert same.mean() >= 0.999, same.mean()
+        # the moves left the 8-wide top level stale (the walk read the packed one); preparing again
+        # rebuilds it from the moved records, and the walk through it returns the same records
+        scene.prepare("wide8")
+        again = engine.trace(scene, torch.from_numpy(rays).cuda(), A.CLOSEST, "wide8").cpu().numpy().view(np.uint32)
+        assert np.array_equal(again, w8)
     finally:
         scene.release()
