@@ -411,13 +411,15 @@ template <int SS, int BLOCK>
 struct W8GroupStack {
   uint2* col;
   static constexpr uint32_t cap = SS;
-  RT_DEV uint2& operator[](uint32_t i) const { return col[i * BLOCK]; }
+  RT_DEV void push(uint32_t& sp, uint2 v) { col[sp++ * BLOCK] = v; }
+  RT_DEV uint2 pop(uint32_t& sp) { return col[--sp * BLOCK]; }
 };
 template <int BLOCK>
 struct W8GroupStack<0, BLOCK> {
   uint2 e[W8_STACK];
   static constexpr uint32_t cap = W8_STACK;
-  RT_DEV uint2& operator[](uint32_t i) { return e[i]; }
+  RT_DEV void push(uint32_t& sp, uint2 v) { e[sp++] = v; }
+  RT_DEV uint2 pop(uint32_t& sp) { return e[--sp]; }
 };
 
 template <uint32_t LAYOUT, int AM, bool COUNT, bool LAZY, class Stack>
@@ -447,7 +449,7 @@ RT_DEV bool w8_node(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, 
   const uint32_t inner = oct_permute(hits & imask, R.oct);
   if (inner) {
     if (L.g_bits) {
-      if (L.sp < Stack::cap) stack[L.sp++] = make_uint2(L.g_base, L.g_bits | L.g_imask << 8);
+      if (L.sp < Stack::cap) stack.push(L.sp, make_uint2(L.g_base, L.g_bits | L.g_imask << 8));
       else atomicAdd(&st->stack_drops, 1ull);
     }
     L.g_base = child_base, L.g_bits = inner, L.g_imask = imask;
@@ -461,7 +463,7 @@ template <class Stack>
 RT_DEV bool w8_next(W8Lane& L, Stack& stack) {
   while (L.g_bits == 0) {
     if (L.sp == 0) return false;
-    const uint2 e = stack[--L.sp];
+    const uint2 e = stack.pop(L.sp);
     L.g_base = e.x, L.g_bits = e.y & 0xffu, L.g_imask = e.y >> 8;
   }
   const uint32_t k = __ffs(L.g_bits) - 1;
