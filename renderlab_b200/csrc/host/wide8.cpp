@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <numeric>
+#include <queue>
 #include <thread>
 #include <array>
 
@@ -50,7 +51,9 @@ class Binary {
     init(std::move(boxes));
   }
   explicit Binary(std::vector<Aabb> boxes) { init(std::move(boxes)); }
-  int build() { return node(0, (uint32_t)ref_.size()); }
+  // `fork_levels`: the top levels whose right subtrees are built by threads of their own (subtrees
+  // of at least FORK_MIN primitives). The tree is the same as a serial build's, node for node.
+  int build(int fork_levels = 0) { return node(0, (uint32_t)ref_.size(), nodes_, fork_levels); }
   const std::vector<BNode>& nodes() const { return nodes_; }
   const std::vector<uint32_t>& refs() const { return ref_; }
 
@@ -69,18 +72,22 @@ class Binary {
   std::vector<uint32_t> ref_;
   std::vector<BNode> nodes_;
 
-  int leaf(uint32_t first, uint32_t n, const Aabb& b) {
-    nodes_.push_back(BNode{b, {-1, -1}, first, n});
-    return (int)nodes_.size() - 1;
+  static constexpr uint32_t FORK_MIN = 1u << 15;
+
+  static int leaf(std::vector<BNode>& out, uint32_t first, uint32_t n, const Aabb& b) {
+    out.push_back(BNode{b, {-1, -1}, first, n});
+    return (int)out.size() - 1;
   }
 
-  int node(uint32_t first, uint32_t n) {
+  // Builds the subtree over refs [first, first + n) into `out`, in preorder (a node before its
+  // left subtree, the left subtree before the right). Threads touch disjoint ref ranges.
+  int node(uint32_t first, uint32_t n, std::vector<BNode>& out, int fork) {
     Aabb b = Aabb::empty(), cb = Aabb::empty();
     for (uint32_t k = first; k < first + n; ++k) {
       b.grow(box_[ref_[k]]);
       cb.grow(&cen_[3 * (size_t)ref_[k]]);
     }
-    if (n == 1) return leaf(first, n, b);
+    if (n == 1) return leaf(out, first, n, b);
     // binned SAH over the centroid bounds, all three axes
     double best = INFINITY;
     int best_axis = -1, best_bin = 0;
@@ -118,7 +125,7 @@ class Binary {
         if (c < best) best = c, best_axis = a, best_bin = k;
       }
     }
-    if (n <= W8_MAX_LEAF && (best_axis < 0 || COST_TRI * n <= best)) return leaf(first, n, b);
+    if (n <= W8_MAX_LEAF && (best_axis < 0 || COST_TRI * n <= best)) return leaf(out, first, n, b);
     uint32_t mid;
     if (best_axis >= 0) {
       const float ext = cb.hi[best_axis] - cb.lo[best_axis], scale = (float)BINS / ext, lo = cb.lo[best_axis];
@@ -129,15 +136,37 @@ class Binary {
     } else {
       mid = first + n / 2;  // coincident centroids: split the list
     }
-    const int me = (int)nodes_.size();
-    nodes_.push_back(BNode{b, {-1, -1}, 0, 0});
-    const int l = node(first, mid - first);
-    const int r = node(mid, first + n - mid);
-    nodes_[me].kid[0] = l;
-    nodes_[me].kid[1] = r;
+    const int me = (int)out.size();
+    out.push_back(BNode{b, {-1, -1}, 0, 0});
+    int l, r;
+    if (fork > 0 && first + n - mid >= FORK_MIN && mid - first >= FORK_MIN) {
+      std::vector<BNode> right;
+      int rr = 0;
+      std::thread t([&] { rr = node(mid, first + n - mid, right, fork - 1); });
+      l = node(first, mid - first, out, fork - 1);
+      t.join();
+      const int base = (int)out.size();
+      for (BNode x : right) {
+        if (x.kid[0] >= 0) x.kid[0] += base, x.kid[1] += base;
+        out.push_back(x);
+      }
+      r = rr + base;
+    } else {
+      l = node(first, mid - first, out, fork);
+      r = node(mid, first + n - mid, out, fork);
+    }
+    out[me].kid[0] = l;
+    out[me].kid[1] = r;
     return me;
   }
 };
+
+// Levels of a binary build that fork their right subtrees, for about `threads` threads at once.
+int fork_levels(int threads) {
+  int levels = 0;
+  while (levels < 6 && (2 << levels) <= threads) ++levels;
+  return levels;
+}
 
 // Smallest power-of-two exponent e with 255 * 2^e >= ext (a normal float scale).
 int scale_exponent(double ext) {
@@ -330,11 +359,11 @@ void emit_wide8(std::vector<BNode>& bn, int broot, const std::vector<uint32_t>& 
 
 }  // namespace
 
-void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
+void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out, int threads) {
   out = Wide8Blas{};
   if (tris.empty()) return;
   Binary bin(tris);
-  const int broot = bin.build();
+  const int broot = bin.build(fork_levels(threads));
   std::vector<BNode> bn = bin.nodes();
   struct TriLeaf {
     const std::vector<SrcTri>& tris;
@@ -351,11 +380,11 @@ void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out) {
   emit_wide8(bn, broot, bin.refs(), out.nodes, out.max_exponent, out.depth, leaf);
 }
 
-void build_wide8_top(const std::vector<Aabb>& boxes, Wide8Top& out) {
+void build_wide8_top(const std::vector<Aabb>& boxes, Wide8Top& out, int threads) {
   out = Wide8Top{};
   if (boxes.empty()) return;
   Binary bin(boxes);
-  const int broot = bin.build();
+  const int broot = bin.build(fork_levels(threads));
   std::vector<BNode> bn = bin.nodes();
   struct InstanceLeaf {
     std::vector<uint32_t>& items;
@@ -455,7 +484,7 @@ bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8
       if (b >= nb) break;
       std::vector<SrcTri> tris;
       gather(layout, w, first_rec[b], tris);
-      build_wide8(tris, built[b]);
+      build_wide8(tris, built[b], std::max(1, threads / (int)nb));
     }
   };
   const int nt = std::max(1, std::min<int>(threads, (int)nb));
@@ -497,36 +526,199 @@ bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8
     out.inst[2 * i + 1] = tri_base[blas_of[i]];
   }
   out.blas_count = nb;
-  build_wide8_top_of(layout, w, out.top_nodes, out.top_items, &out.top_depth);
+  build_wide8_top_of(layout, w, out.nodes, out.inst, out.top_nodes, out.top_items, &out.top_depth);
   return true;
 }
 
-bool build_wide8_top_of(uint32_t layout, const uint32_t* w, std::vector<uint32_t>& nodes, std::vector<uint32_t>& items,
-                        uint32_t* depth) {
+namespace {
+
+// Object-space box of an 8-wide node: the union of its non-empty children's boxes, exact.
+bool node_box(const uint32_t* n, double lo[3], double hi[3]) {
+  bool any = false;
+  for (int a = 0; a < 3; ++a) lo[a] = INFINITY, hi[a] = -INFINITY;
+  for (int s = 0; s < 8; ++s) {
+    const uint32_t meta = ((s < 4 ? n[6] : n[7]) >> (8 * (s & 3))) & 255u;
+    if (!((n[3] >> (24 + s)) & 1u) && meta == 0) continue;  // empty
+    any = true;
+    for (int a = 0; a < 3; ++a) {
+      const int e = (int)((n[3] >> (8 * a)) & 255u) - 127;
+      const uint32_t ql = (n[8 + 2 * a + (s >> 2)] >> (8 * (s & 3))) & 255u;
+      const uint32_t qh = (n[8 + 2 * (3 + a) + (s >> 2)] >> (8 * (s & 3))) & 255u;
+      lo[a] = std::min(lo[a], (double)as_float(n[a]) + std::ldexp((double)ql, e));
+      hi[a] = std::max(hi[a], (double)as_float(n[a]) + std::ldexp((double)qh, e));
+    }
+  }
+  return any;
+}
+
+// The inverse of the affine map whose rows are a[0..11] (an instance's world-to-object rows):
+// the object-to-world map, in double. False when it is singular or not finite.
+bool affine_inverse(const double* a, double* m) {
+  const double c00 = a[5] * a[10] - a[6] * a[9], c01 = a[2] * a[9] - a[1] * a[10], c02 = a[1] * a[6] - a[2] * a[5];
+  const double c10 = a[6] * a[8] - a[4] * a[10], c11 = a[0] * a[10] - a[2] * a[8], c12 = a[2] * a[4] - a[0] * a[6];
+  const double c20 = a[4] * a[9] - a[5] * a[8], c21 = a[1] * a[8] - a[0] * a[9], c22 = a[0] * a[5] - a[1] * a[4];
+  const double det = a[0] * c00 + a[1] * c10 + a[2] * c20;
+  if (!std::isfinite(det) || det == 0.0) return false;
+  const double r[9] = {c00 / det, c01 / det, c02 / det, c10 / det, c11 / det, c12 / det, c20 / det, c21 / det, c22 / det};
+  bool ok = true;
+  for (int i = 0; i < 3; ++i) {
+    for (int j = 0; j < 3; ++j) m[4 * i + j] = r[3 * i + j];
+    m[4 * i + 3] = -(r[3 * i] * a[3] + r[3 * i + 1] * a[7] + r[3 * i + 2] * a[11]);
+    for (int j = 0; j < 4; ++j) ok = ok && std::isfinite(m[4 * i + j]);
+  }
+  return ok;
+}
+
+double inf_norm(const double* m) {
+  double n = 0.0;
+  for (int i = 0; i < 3; ++i) n = std::max(n, std::fabs(m[4 * i]) + std::fabs(m[4 * i + 1]) + std::fabs(m[4 * i + 2]));
+  return n;
+}
+
+// One leaf of the re-braided top level: instance `inst` entered at its BLAS node `node` (global
+// index), with the world box of that node's subtree.
+struct Entry {
+  uint32_t inst, node;
+  double lo[3], hi[3];
+  double area() const {
+    const double x = hi[0] - lo[0], y = hi[1] - lo[1], z = hi[2] - lo[2];
+    return x * y + y * z + z * x;
+  }
+};
+
+}  // namespace
+
+bool instance_model(const uint32_t* rows, double* m) {
+  double a[12];
+  for (int k = 0; k < 12; ++k) a[k] = as_float(rows[k]);
+  return affine_inverse(a, m);
+}
+
+bool entry_object_box(const uint32_t* node, double* lo, double* hi) { return node_box(node, lo, hi); }
+
+void entry_world_box(const double* m, const double* olo, const double* ohi, double* lo, double* hi) {
+  for (int a = 0; a < 3; ++a) lo[a] = INFINITY, hi[a] = -INFINITY;
+  for (int c = 0; c < 8; ++c) {
+    const double p[3] = {c & 1 ? ohi[0] : olo[0], c & 2 ? ohi[1] : olo[1], c & 4 ? ohi[2] : olo[2]};
+    for (int a = 0; a < 3; ++a) {
+      const double x = m[4 * a] * p[0] + m[4 * a + 1] * p[1] + m[4 * a + 2] * p[2] + m[4 * a + 3];
+      lo[a] = std::min(lo[a], x), hi[a] = std::max(hi[a], x);
+    }
+  }
+}
+
+bool build_wide8_top_of(uint32_t layout, const uint32_t* w, const std::vector<uint32_t>& blas_nodes,
+                        const std::vector<uint32_t>& inst, std::vector<uint32_t>& nodes, std::vector<uint32_t>& items,
+                        uint32_t* depth, uint32_t per_instance) {
   nodes.clear(), items.clear();
   const uint32_t count = w[0];
   if (w[1] == 0 || count < 2) return false;  // a flat instance list: the walk loops over it
   const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
-  std::vector<Aabb> boxes;
-  std::vector<uint32_t> which;
+  const size_t n_blas_nodes = blas_nodes.size() / W8_NODE_WORDS;
+  // the instances the walk may enter: a usable record world box (the reference's top level culls
+  // every other one) and a non-empty BLAS
+  std::vector<uint32_t> live;
+  double scene_abs = 0.0;
   for (uint32_t i = 0; i < count; ++i) {
     const uint32_t* r = w + header + stride * (size_t)i;
-    Aabb b;
-    bool ok = true;
+    bool ok = 2 * (size_t)i + 1 < inst.size() && inst[2 * i] < n_blas_nodes;
     for (int a = 0; a < 3; ++a) {
-      b.lo[a] = as_float(r[12 + a]), b.hi[a] = as_float(r[15 + a]);
-      ok = ok && std::isfinite(b.lo[a]) && std::isfinite(b.hi[a]) && b.lo[a] <= b.hi[a];
+      const float l = as_float(r[12 + a]), h = as_float(r[15 + a]);
+      ok = ok && std::isfinite(l) && std::isfinite(h) && l <= h;
     }
-    if (ok) boxes.push_back(b), which.push_back(i);
+    if (!ok) continue;
+    live.push_back(i);
+    for (int a = 0; a < 3; ++a)
+      scene_abs = std::max({scene_abs, std::fabs((double)as_float(r[12 + a])), std::fabs((double)as_float(r[15 + a]))});
   }
-  if (boxes.empty()) return false;
+  if (live.empty()) return false;
+  // Per instance its object-to-world map and the map's condition (|M| |M^-1|, infinity norms).
+  std::vector<std::array<double, 12>> model(count);
+  std::vector<double> cond(count, 0.0);
+  std::vector<uint8_t> mapped(count, 0);
+  std::vector<Entry> entries;
+  entries.reserve(std::min<size_t>((size_t)per_instance * live.size(), W8_BRAID_MAX) + 8);
+  auto world_of = [&](uint32_t i, uint32_t node, Entry& e) {
+    double olo[3], ohi[3];
+    if (!node_box(&blas_nodes[(size_t)node * W8_NODE_WORDS], olo, ohi)) return false;
+    entry_world_box(model[i].data(), olo, ohi, e.lo, e.hi);
+    // Margin for the rounding of the walk's f32 object-space ray: the world ray passes within
+    // about 12 u |M| |M^-1| (|o| + |hit|) of M p when the f32 object ray meets object point p
+    // (u = 2^-24); 2^-16 of the scene's extent covers rays starting within about 20 extents.
+    const double pad = W8_BRAID_PAD * cond[i] * (scene_abs + std::max({e.hi[0] - e.lo[0], e.hi[1] - e.lo[1], e.hi[2] - e.lo[2]}));
+    for (int a = 0; a < 3; ++a) e.lo[a] -= pad, e.hi[a] += pad;
+    e.inst = i, e.node = node;
+    return std::isfinite(e.lo[0] + e.lo[1] + e.lo[2] + e.hi[0] + e.hi[1] + e.hi[2]);
+  };
+  struct Open {
+    double area;
+    size_t at;
+    bool operator<(const Open& o) const { return area < o.area; }
+  };
+  std::priority_queue<Open> open;
+  for (uint32_t i : live) {
+    const uint32_t* r = w + header + stride * (size_t)i;
+    double rows[12];
+    for (int k = 0; k < 12; ++k) rows[k] = as_float(r[k]);
+    Entry e;
+    if (affine_inverse(rows, model[i].data())) {
+      mapped[i] = 1;
+      cond[i] = inf_norm(model[i].data()) * inf_norm(rows);
+      if (world_of(i, inst[2 * i], e)) {
+        entries.push_back(e);
+        open.push({e.area(), entries.size() - 1});
+        continue;
+      }
+      mapped[i] = 0;
+    }
+    // no usable object-to-world map: the instance whole, under its record world box
+    e.inst = i, e.node = inst[2 * i];
+    for (int a = 0; a < 3; ++a) e.lo[a] = as_float(r[12 + a]), e.hi[a] = as_float(r[15 + a]);
+    entries.push_back(e);
+  }
+  // Re-braiding (Benthin, Woop, Wald and Afra 2017, "Improved Two-Level BVHs using Partial
+  // Re-Braiding"): the entry with the largest world box is replaced by its node's children while
+  // the budget lasts. Only nodes whose children are all inner nodes open, so the entries of an
+  // instance stay an exact cut of its BLAS: every triangle under exactly one entry.
+  const size_t budget = std::min<size_t>((size_t)per_instance * live.size(), std::max<size_t>(live.size(), W8_BRAID_MAX));
+  while (!open.empty() && entries.size() < budget) {
+    const Open top = open.top();
+    open.pop();
+    const Entry e = entries[top.at];
+    const uint32_t* n = &blas_nodes[(size_t)e.node * W8_NODE_WORDS];
+    const uint32_t imask = n[3] >> 24;
+    if (n[6] != 0 || n[7] != 0 || __builtin_popcount(imask) < 2) continue;  // has leaves, or one child
+    Entry kids[8];
+    int nk = 0;
+    bool ok = true;
+    for (int s = 0; s < 8 && ok; ++s)
+      if ((imask >> s) & 1u) ok = world_of(e.inst, n[4] + (uint32_t)__builtin_popcount(imask & ((1u << s) - 1u)), kids[nk++]);
+    if (!ok) continue;
+    entries[top.at] = kids[0];
+    open.push({kids[0].area(), top.at});
+    for (int k = 1; k < nk; ++k) {
+      entries.push_back(kids[k]);
+      open.push({kids[k].area(), entries.size() - 1});
+    }
+  }
+  std::vector<Aabb> boxes(entries.size());
+  for (size_t k = 0; k < entries.size(); ++k)
+    for (int a = 0; a < 3; ++a) {  // rounded outward to f32
+      float l = (float)entries[k].lo[a], h = (float)entries[k].hi[a];
+      if ((double)l > entries[k].lo[a]) l = std::nextafter(l, -INFINITY);
+      if ((double)h < entries[k].hi[a]) h = std::nextafter(h, INFINITY);
+      boxes[k].lo[a] = l, boxes[k].hi[a] = h;
+    }
   Wide8Top top;
-  build_wide8_top(boxes, top);
+  build_wide8_top(boxes, top, (int)std::max(1u, std::thread::hardware_concurrency()));
   // the walk's top stack holds a group entry a level plus one node's eight leaves
   if (top.max_exponent > W8_MAX_EXPONENT || top.depth + 9 > W8_TOP_STACK) return false;
-  for (uint32_t& it : top.items) it = which[it];
+  items.resize(2 * top.items.size());
+  for (size_t k = 0; k < top.items.size(); ++k) {
+    const Entry& e = entries[top.items[k]];
+    items[2 * k] = e.inst, items[2 * k + 1] = e.node - inst[2 * e.inst];
+  }
   nodes = std::move(top.nodes);
-  items = std::move(top.items);
   if (depth) *depth = top.depth;
   return true;
 }

@@ -54,13 +54,15 @@ struct Wide8Scene {
   size_t blas_count = 0;
   uint32_t depth = 0;  // the deepest BLAS's levels
   // the 8-wide top level (empty: the scene is a flat instance list, or keeps its BVH4 top level)
+  // and its leaves' entries, two words each: instance, node of the instance's BLAS to enter at
+  // (relative to the BLAS's root)
   std::vector<uint32_t> top_nodes, top_items;
   uint32_t top_depth = 0;
 };
 
-// An 8-wide top level over instance world boxes, in the BLAS node format: a leaf slot's `count`
-// items (one: W8_MAX_LEAF) are instance indices at items[node word 5 + offset]; node 0 is the root
-// and nodes are numbered breadth first, so the upper levels are the lowest node indices.
+// An 8-wide top level in the BLAS node format: a leaf slot's `count` items (one: W8_MAX_LEAF) are
+// at items[node word 5 + offset]; node 0 is the root and nodes are numbered breadth first, so the
+// upper levels are the lowest node indices.
 struct Wide8Top {
   std::vector<uint32_t> nodes;
   std::vector<uint32_t> items;
@@ -74,27 +76,56 @@ struct SrcTri {
   uint32_t ident, ref;
 };
 
-void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out);
+// `threads`: about how many threads the build may use (large subtrees are built concurrently;
+// the tree does not depend on it).
+void build_wide8(const std::vector<SrcTri>& tris, Wide8Blas& out, int threads = 1);
 struct Aabb;
-void build_wide8_top(const std::vector<Aabb>& boxes, Wide8Top& out);
+void build_wide8_top(const std::vector<Aabb>& boxes, Wide8Top& out, int threads = 1);
 // Entries of the WIDE8 walk's top-level stack (pairs of words): a level's group, plus one node's
-// eight instance leaves.
+// eight leaves.
 constexpr uint32_t W8_TOP_STACK = 32;
-// The 8-wide top level of a packed scene's instances (over the world boxes of its records, words
-// 12-17), when it has a top level; false (nothing built) for a flat instance list, or when the
-// instances span more than the node scale allows or the tree is too deep for the walk's stack:
-// the walk then uses the packed BVH4 top level.
-bool build_wide8_top_of(uint32_t layout, const uint32_t* words, std::vector<uint32_t>& nodes,
-                        std::vector<uint32_t>& items, uint32_t* depth = nullptr);
+// The re-braided top level's size: at most this many leaves per instance, and in all (at least one
+// per instance), and the relative margin of its world boxes.
+#ifndef RT_W8_BRAID
+#define RT_W8_BRAID 256
+#endif
+constexpr uint32_t W8_BRAID_PER_INSTANCE = RT_W8_BRAID;
+constexpr size_t W8_BRAID_MAX = size_t(1) << 22;
+constexpr double W8_BRAID_PAD = 1.0 / 65536.0;
+// The 8-wide top level of a packed scene with a top level, over its built 8-wide BLAS nodes and
+// instance table (Wide8Scene::nodes, ::inst). Its leaves are entries (instance, BLAS node): each
+// instance starts as one entry at its BLAS root, and the entry with the largest world box is
+// replaced by its node's children -- nodes whose children are all inner nodes only, so an
+// instance's entries always cover each of its triangles exactly once -- until there are
+// `per_instance` entries per instance (Benthin, Woop, Wald and Afra 2017, partial re-braiding).
+// An entry's world box bounds its node's box under the instance's object-to-world map (the
+// inverse of the record's rows, in double), with a margin for the walk's f32 object-space ray.
+// Instances without a usable record world box are left out (the reference's top level never
+// enters them); one whose rows cannot be inverted is one entry under its record world box.
+// False (nothing built) for a flat instance list, or when the entries span more than the node
+// scale allows or the tree is too deep for the walk's stack: the walk then uses the packed BVH4
+// top level.
+bool build_wide8_top_of(uint32_t layout, const uint32_t* words, const std::vector<uint32_t>& blas_nodes,
+                        const std::vector<uint32_t>& inst, std::vector<uint32_t>& nodes, std::vector<uint32_t>& items,
+                        uint32_t* depth = nullptr, uint32_t per_instance = W8_BRAID_PER_INSTANCE);
+// An instance's object-to-world map (3 rows of 4): the inverse of its record's world-to-object rows
+// (12 f32 words), in double; false when they cannot be inverted.
+bool instance_model(const uint32_t* rows, double* m);
+// The box of a BLAS node's subtree: the union of its children's boxes, exact; false when it has none.
+bool entry_object_box(const uint32_t* node, double* lo, double* hi);
+// The box of the eight corners of the object box [olo, ohi] under the affine map m (3 rows of 4).
+void entry_world_box(const double* m, const double* olo, const double* ohi, double* lo, double* hi);
 bool build_wide8_scene(uint32_t layout, const uint32_t* words, size_t n_words, Wide8Scene& out, std::string& err,
                        int threads);
 // Checks a built layout (wide8_check.cpp): ranges, one leaf per triangle, every child box
 // enclosing its child in exact arithmetic, inverted empty slots, the recorded depth. info: nodes,
 // triangles, depth, distinct BLAS.
 bool check_wide8_scene(const Wide8Scene& s, uint32_t info[4], std::string& err);
-// Checks the 8-wide top level of a scene built from `words`: every instance with a usable world
-// box in exactly one leaf, every child box enclosing the world boxes below it, nodes after their
-// parents, the recorded depth within the walk's stack.
+// Checks the 8-wide top level of a scene built from `words`: each instance with a usable world
+// box and a non-empty BLAS has entries that cut its BLAS exactly (every triangle under exactly one
+// entry), every leaf box encloses its entry's node box under the instance's object-to-world map
+// (or the record world box, for rows that cannot be inverted), every inner child box the boxes
+// below it, nodes after their parents, the recorded depth within the walk's stack.
 bool check_wide8_top(uint32_t layout, const uint32_t* words, const Wide8Scene& s, std::string& err);
 
 }  // namespace rtb

@@ -92,11 +92,31 @@ bool check_node(const Wide8Scene& s, uint32_t node, uint32_t level, std::vector<
   return true;
 }
 
-// The same for a node of the 8-wide top level: its leaves hold instance indices, and a child box
-// must enclose the world boxes (record words 12-17) of the instances below it.
+// The box a top-level leaf must enclose for entry (instance i, BLAS node `rel` below its root):
+// the node's box under the instance's object-to-world map, or the record world box when the
+// record's rows cannot be inverted.
+bool entry_box(const Wide8Scene& s, const uint32_t* r, uint32_t i, uint32_t rel, double* lo, double* hi,
+               std::string& err) {
+  const size_t nn = s.nodes.size() / W8_NODE_WORDS;
+  if (s.inst[2 * i] >= nn || rel >= nn - s.inst[2 * i]) return err = "a top-level entry names no node of its BLAS", false;
+  double m[12];
+  if (!instance_model(r, m)) {
+    for (int a = 0; a < 3; ++a) lo[a] = as_float(r[12 + a]), hi[a] = as_float(r[15 + a]);
+    return true;
+  }
+  double olo[3], ohi[3];
+  if (!entry_object_box(&s.nodes[(size_t)(s.inst[2 * i] + rel) * W8_NODE_WORDS], olo, ohi))
+    return err = "a top-level entry's node has no children", false;
+  entry_world_box(m, olo, ohi, lo, hi);
+  return true;
+}
+
+// The same for a node of the 8-wide top level: its leaves hold entries (instance, BLAS node), and
+// a child box must enclose the world boxes of the entries below it. Collects each instance's
+// entries.
 bool check_top_node(const Wide8Scene& s, const uint32_t* words, size_t header, size_t stride, uint32_t count,
-                    uint32_t node, uint32_t level, std::vector<uint8_t>& seen_node, std::vector<uint8_t>& seen_inst,
-                    uint32_t& depth, Extent& ext, std::string& err) {
+                    uint32_t node, uint32_t level, std::vector<uint8_t>& seen_node,
+                    std::vector<std::vector<uint32_t>>& entries, uint32_t& depth, Extent& ext, std::string& err) {
   const size_t nn = s.top_nodes.size() / W8_NODE_WORDS;
   if (node >= nn) return err = "top-level node index out of range", false;
   if (seen_node[node]) return err = "a top-level node is reached twice", false;
@@ -121,23 +141,34 @@ bool check_top_node(const Wide8Scene& s, const uint32_t* words, size_t header, s
     if (inner) {
       const uint32_t c = child_base + (uint32_t)__builtin_popcount(imask & ((1u << slot) - 1u));
       if (c <= node) return err = "top-level child not after its parent", false;
-      if (!check_top_node(s, words, header, stride, count, c, level + 1, seen_node, seen_inst, depth, child, err)) return false;
+      if (!check_top_node(s, words, header, stride, count, c, level + 1, seen_node, entries, depth, child, err)) return false;
     } else {
       for (uint32_t k = 0; k < (meta >> 5); ++k) {
         const size_t at = (size_t)item_base + (meta & 31u) + k;
-        if (at >= s.top_items.size()) return err = "top-level item out of range", false;
-        const uint32_t i = s.top_items[at];
+        if (2 * at + 1 >= s.top_items.size()) return err = "top-level item out of range", false;
+        const uint32_t i = s.top_items[2 * at], rel = s.top_items[2 * at + 1];
         if (i >= count) return err = "top-level leaf names no instance", false;
-        if (seen_inst[i]++) return err = "an instance is in two top-level leaves", false;
-        const uint32_t* r = words + header + stride * (size_t)i;
         double l[3], h[3];
-        for (int a = 0; a < 3; ++a) l[a] = as_float(r[12 + a]), h[a] = as_float(r[15 + a]);
+        if (!entry_box(s, words + header + stride * (size_t)i, i, rel, l, h, err)) return false;
+        entries[i].push_back(rel);
         child.grow(l, h);
       }
     }
-    if (!child.within(lo, hi)) return err = "a top-level child box does not enclose its instances' world boxes", false;
+    if (!child.within(lo, hi)) return err = "a top-level child box does not enclose its entries' world boxes", false;
     ext.grow(child.lo, child.hi);
   }
+  return true;
+}
+
+// Whether the entries `cut` (sorted node indices below the BLAS root `base`) cut the BLAS at
+// `node` exactly: `node` is an entry, or has no leaf slots and each of its inner children is cut.
+bool cuts(const Wide8Scene& s, uint32_t base, uint32_t node, const std::vector<uint32_t>& cut, size_t& used) {
+  if (std::binary_search(cut.begin(), cut.end(), node - base)) return ++used, true;
+  const uint32_t* w = &s.nodes[(size_t)node * W8_NODE_WORDS];
+  if (w[6] != 0 || w[7] != 0) return false;  // leaf triangles above every entry: no entry holds them
+  const uint32_t imask = w[3] >> 24;
+  for (int k = 0; k < __builtin_popcount(imask); ++k)
+    if (!cuts(s, base, w[4] + (uint32_t)k, cut, used)) return false;
   return true;
 }
 
@@ -147,19 +178,31 @@ bool check_wide8_top(uint32_t layout, const uint32_t* words, const Wide8Scene& s
   if (s.top_nodes.empty()) return true;  // no 8-wide top level: the walk uses the packed one
   const uint32_t count = words[0];
   const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
-  std::vector<uint8_t> seen_node(s.top_nodes.size() / W8_NODE_WORDS, 0), seen_inst(count, 0);
+  if (s.inst.size() < 2 * (size_t)count) return err = "instance table shorter than the records", false;
+  std::vector<uint8_t> seen_node(s.top_nodes.size() / W8_NODE_WORDS, 0);
+  std::vector<std::vector<uint32_t>> entries(count);
   uint32_t depth = 0;
   Extent ext;
-  if (!check_top_node(s, words, header, stride, count, 0, 1, seen_node, seen_inst, depth, ext, err)) return false;
+  if (!check_top_node(s, words, header, stride, count, 0, 1, seen_node, entries, depth, ext, err)) return false;
   if (std::find(seen_node.begin(), seen_node.end(), 0) != seen_node.end()) return err = "an unreachable top-level node", false;
   for (uint32_t i = 0; i < count; ++i) {
     const uint32_t* r = words + header + stride * (size_t)i;
-    bool valid = true;
+    bool valid = s.inst[2 * i] != EMPTY;
     for (int a = 0; a < 3; ++a) {
       const float l = as_float(r[12 + a]), h = as_float(r[15 + a]);
       valid = valid && std::isfinite(l) && std::isfinite(h) && l <= h;
     }
-    if (valid && !seen_inst[i]) return err = "an instance no top-level leaf holds", false;
+    std::vector<uint32_t>& cut = entries[i];
+    if (!valid) {
+      if (!cut.empty()) return err = "a top-level entry for an instance the walk must not enter", false;
+      continue;
+    }
+    if (cut.empty()) return err = "an instance no top-level leaf holds", false;
+    std::sort(cut.begin(), cut.end());
+    if (std::adjacent_find(cut.begin(), cut.end()) != cut.end()) return err = "an entry is in two top-level leaves", false;
+    size_t used = 0;
+    if (!cuts(s, s.inst[2 * i], s.inst[2 * i], cut, used) || used != cut.size())
+      return err = "an instance's entries do not cut its BLAS exactly", false;
   }
   if (depth != s.top_depth || depth + 9 > W8_TOP_STACK) return err = "top-level depth differs from the record or the walk's stack", false;
   return true;

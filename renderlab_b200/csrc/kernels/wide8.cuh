@@ -58,7 +58,8 @@ struct W8View {
   const uint4* tris;      // 3 uint4 a triangle
   const uint32_t* inst;   // 2 words an instance: node base, triangle base
   // the 8-wide top level (null: walk the packed BVH4 top level), breadth first from its root, and
-  // its leaves' instance indices
+  // its leaves' entries, two words each: instance, node of the instance's BLAS to enter at
+  // (relative to the BLAS's root)
   const uint4* top = nullptr;
   const uint32_t* top_items = nullptr;
   uint32_t top_count = 0;
@@ -66,10 +67,15 @@ struct W8View {
 
 // Top-level nodes staged in shared memory by every block of the per-ray walk (the first levels,
 // which every ray reads): 64 nodes, 5 KB.
-constexpr uint32_t W8_TOP_CACHE = 64;
+#ifndef RT_W8_TOP_CACHE
+#define RT_W8_TOP_CACHE 64
+#endif
+constexpr uint32_t W8_TOP_CACHE = RT_W8_TOP_CACHE;
 // Pairs of words in the per-ray walk's 8-wide top-level stack: a group entry (first child node,
-// pending bits | inner mask << 8) a level, and one node's leaf instances (instance, 0).
+// pending bits | inner mask << 8) a level, and one node's leaf entries (instance, BLAS node |
+// W8_ENTRY).
 constexpr uint32_t W8_TOP_STACK = 32;
+constexpr uint32_t W8_ENTRY = 0x80000000u;
 
 struct W8Best {
   float t;          // f32 t of the best candidate (f32(t64) once re-tested)
@@ -475,12 +481,14 @@ RT_DEV bool w8_next(W8Lane& L, Stack& stack) {
 
 // Enters instance i when its world box survives; sets up the object-space ray.
 template <uint32_t LAYOUT, int AM, bool COUNT, bool LAZY = false>
-// `from_top`: the instance comes from a top-level leaf, whose box the walk has just tested. That
-// box is the instance's world box, so its test here could only pass: the walk skips it (WIDE8's
-// results do not depend on which extra instances it enters, only its work does). A flat instance
-// list has no such test, so there the world box is tested here.
+// `from_top`: the instance comes from a leaf of the 8-wide top level, whose box the walk has just
+// tested: a box around the world positions of the subtree of BLAS node `at` (relative to the root),
+// where this entry starts the walk. The instance's world box would not cull anything more that
+// the walk would find (WIDE8's results do not depend on which extra instances it enters, only its
+// work does), so it is not tested. A flat instance list has no top-level test, so there the world
+// box is tested here.
 RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L, uint32_t i, unsigned long long* cnt,
-                     bool from_top) {
+                     bool from_top, uint32_t at = 0) {
   const size_t r = (LAYOUT == 0 ? 16 : 8) + (size_t)(LAYOUT == 0 ? 32 : 24) * i;  // 16-byte aligned records
   if (any_of<AM>(L) && (LAYOUT == 0 ? (ld(w, r + 27) & 1u) != 0 : ld(w, r + 22) != 0)) return;
   w8_count<COUNT>(cnt, W8C_INSTANCE_TESTS);
@@ -501,7 +509,7 @@ RT_DEV void w8_enter(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L,
   if (!L.R.valid) return;
   if (!LAZY) w8_shear(w, r, L.ray.o, L.R);
   L.inst = i;
-  L.node = root;
+  L.node = root + at;
   L.g_bits = 0;
   L.sp = 0;
   L.phase = 2;
@@ -641,8 +649,8 @@ RT_DEV uint32_t octant_of(const F3& d) {
 
 // One node of the 8-wide top level (world space): its children's quantised boxes against the
 // world ray and the lane's bound. The inner children met become one group entry; each leaf met
-// pushes its instance above it, the first in visiting order on top, so a node's instances are
-// entered before the walk goes deeper.
+// pushes its entry (instance, BLAS node) above it, the first in visiting order on top, so a node's
+// entries are entered before the walk goes deeper.
 template <bool COUNT>
 RT_DEV void w8_top_node(const W8View& V, const uint4* cache, uint32_t cached, uint32_t node, const W8Lane& L,
                         uint32_t* tstack, uint32_t& tsp, DevStatus* st, unsigned long long* cnt) {
@@ -674,8 +682,12 @@ RT_DEV void w8_top_node(const W8View& V, const uint4* cache, uint32_t cached, ui
     const uint32_t s = k ^ TW.oct;
     const uint32_t m = ((s < 4 ? a1.z : a1.w) >> (8 * (s & 3))) & 0xffu;
     for (uint32_t j = m >> 5; j-- > 0;) {  // an empty slot met all the same has no items
-      if (tsp + 2 <= 2 * W8_TOP_STACK) tstack[tsp] = __ldg(V.top_items + a1.y + (m & 31u) + j), tstack[tsp + 1] = 0, tsp += 2;
-      else atomicAdd(&st->stack_drops, 1ull);
+      if (tsp + 2 <= 2 * W8_TOP_STACK) {
+        const uint2 e = __ldg(reinterpret_cast<const uint2*>(V.top_items) + a1.y + (m & 31u) + j);
+        tstack[tsp] = e.x, tstack[tsp + 1] = e.y | W8_ENTRY, tsp += 2;
+      } else {
+        atomicAdd(&st->stack_drops, 1ull);
+      }
     }
   }
 }
@@ -764,8 +776,8 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       if (top8) {
         L.tsp -= 2;
         const uint32_t ex = tstack[L.tsp], ey = tstack[L.tsp + 1];
-        if (ey == 0) {  // an instance leaf
-          w8_enter<LAYOUT, AM, COUNT, LAZY>(w, V, L, ex, cnt, true);
+        if (ey & W8_ENTRY) {  // a leaf's entry: an instance, at a node of its BLAS
+          w8_enter<LAYOUT, AM, COUNT, LAZY>(w, V, L, ex, cnt, true, ey & ~W8_ENTRY);
           continue;
         }
         uint32_t bits = ey & 0xffu;  // a group: its first pending child now, the rest back on the stack

@@ -21,7 +21,8 @@ struct SceneView {
   size_t w8_nodes_at, w8_tris_at, w8_inst_at;
   uint32_t w8_depth;  // levels of the deepest 8-wide BLAS
   // The 8-wide top level (null: walk the packed top level): w8_top_nodes 80-byte nodes, breadth
-  // first from the root, then the leaves' instance indices at word w8_top_items_at.
+  // first from the root, then the leaves' entries (instance, BLAS node below the instance's root)
+  // at word w8_top_items_at.
   const void* w8_top = nullptr;
   uint32_t w8_top_nodes = 0;
   size_t w8_top_items_at = 0;

@@ -109,13 +109,46 @@ rt_status upload_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& 
   return RT_OK;
 }
 
-// Rebuilds only the 8-wide top level, from the scene's current records.
+// Rebuilds only the 8-wide top level, from the scene's current records and its built 8-wide
+// BLAS nodes and instance table (read back from the device).
 rt_status prepare_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& words) {
   rtb::Wide8Scene top;
   std::string err;
-  rtb::build_wide8_top_of(scene->layout, words.data(), top.top_nodes, top.top_items, &top.top_depth);
+  top.nodes.resize(scene->w8_tris_at - scene->w8_nodes_at);
+  top.inst.resize(2 * (size_t)words[0]);
+  const uint32_t* d = static_cast<const uint32_t*>(scene->d_wide8);
+  RT_CUDA(ctx, cudaMemcpy(top.nodes.data(), d + scene->w8_nodes_at, top.nodes.size() * 4, cudaMemcpyDeviceToHost));
+  if (!top.inst.empty())
+    RT_CUDA(ctx, cudaMemcpy(top.inst.data(), d + scene->w8_inst_at, top.inst.size() * 4, cudaMemcpyDeviceToHost));
+  rtb::build_wide8_top_of(scene->layout, words.data(), top.nodes, top.inst, top.top_nodes, top.top_items, &top.top_depth);
   if (!rtb::check_wide8_top(scene->layout, words.data(), top, err)) top.top_nodes.clear();  // the packed top level
   return upload_top(ctx, scene, top.top_nodes, top.top_items);
+}
+
+// Frees the scene's derived 8-wide layout (its BLASes, instance table and top level): WIDE8 then
+// needs rt_scene_prepare again.
+void drop_wide8(rt_ctx* ctx, rt_scene* scene) {
+  if (!scene->d_wide8) return;
+  cudaFree(scene->d_wide8);
+  scene->d_wide8 = nullptr;
+  scene->device_bytes -= scene->wide8_bytes;
+  ctx->scene_bytes -= scene->wide8_bytes;
+  scene->wide8_bytes = 0;
+  upload_top(ctx, scene, {}, {});
+}
+
+// Whether two versions of a scene's leading words give the 8-wide layout the same instance
+// table: the same instance count and, per record, the same BLAS words.
+bool same_instances(uint32_t layout, const uint32_t* a, const uint32_t* b) {
+  if (a[0] != b[0]) return false;
+  const size_t header = layout == 0 ? 16 : 8, stride = layout == 0 ? 32 : 24;
+  for (uint32_t i = 0; i < a[0]; ++i) {
+    const uint32_t *ra = a + header + stride * (size_t)i, *rb = b + header + stride * (size_t)i;
+    const bool same = layout == 0 ? std::equal(ra + 18, ra + 23, rb + 18)
+                                  : ((ra[18] ^ rb[18]) & ~3u) == 0 && ((ra[19] ^ rb[19]) & ~3u) == 0 && ra[20] == rb[20];
+    if (!same) return false;
+  }
+  return true;
 }
 
 }  // namespace
@@ -251,11 +284,17 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
   std::vector<uint32_t> all(scene->n_words);
   RT_CUDA(ctx, cudaSetDevice(ctx->device));
   RT_CUDA(ctx, cudaMemcpy(all.data(), scene->d_words, scene->n_words * 4, cudaMemcpyDeviceToHost));
+  // the old records, to tell whether the 8-wide instance table still holds
+  const size_t header = scene->layout == 0 ? 16 : 8, stride = scene->layout == 0 ? 32 : 24;
+  const uint32_t most = std::max(all.empty() ? 0u : all[0], n_words ? words[0] : 0u);
+  const std::vector<uint32_t> before(all.begin(), all.begin() + std::min(all.size(), header + stride * (size_t)most));
   std::copy(words, words + n_words, all.begin());
   rtb::SceneInfo info;
   std::string err;
   if (!rtb::validate_scene(scene->layout, all.data(), all.size(), info, err))
     return fail(ctx, RT_ERR_LAYOUT, "records rejected: %s", err.c_str());
+  // records that name other BLASes, or another instance count, void the 8-wide instance table
+  if (scene->d_wide8 && !same_instances(scene->layout, before.data(), all.data())) drop_wide8(ctx, scene);
   RT_CUDA(ctx, cudaMemcpy(scene->d_words, words, n_words * 4, cudaMemcpyHostToDevice));
   scene->info = info;
   scene->w8_top_valid = false;  // the instances' boxes may have moved: the packed top level until re-prepared
