@@ -104,7 +104,10 @@ typedef struct rt_tuning {
   uint32_t fast_refill;  /* FAST: idle lanes (1-32) a persistent warp waits for before taking more rays */
   uint32_t wide8_refill; /* WIDE8: the same */
   uint32_t wide8_stack;  /* WIDE8: RT_STACK_LOCAL or RT_STACK_SHARED */
-  uint32_t reserved[5];
+  uint32_t wide8_entries; /* WIDE8: leaves per instance (1-1024) of the 8-wide top level that later
+                           * rt_scene_prepare calls build: 1 enters each instance at its BLAS root;
+                           * more split the instances' BLASes into world-space entries (default 256) */
+  uint32_t reserved[4];
 } rt_tuning;
 
 typedef struct rt_ctx rt_ctx;

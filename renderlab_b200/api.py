@@ -94,7 +94,7 @@ class RtRnfPlacement(ctypes.Structure):
 
 class RtTuning(ctypes.Structure):
     _fields_ = [("fast_refill", ctypes.c_uint32), ("wide8_refill", ctypes.c_uint32), ("wide8_stack", ctypes.c_uint32),
-                ("reserved", ctypes.c_uint32 * 5)]
+                ("wide8_entries", ctypes.c_uint32), ("reserved", ctypes.c_uint32 * 4)]
 
 
 EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_error", "rt_get_stats",

@@ -13,6 +13,7 @@
 
 #include "../../include/rt_trace.h"
 #include "host/host.hpp"
+#include "host/wide8.hpp"
 #include "launch.hpp"
 
 // Per BLAS of a scene, what rt_scene_refit needs about its (fixed) topology: its nodes ordered
@@ -75,7 +76,7 @@ struct rt_ctx {
   // many launches may be in flight at once across streams.
   unsigned int* d_counters = nullptr;
   std::atomic<uint64_t> counter_seq{0};
-  rt_tuning tuning = {8, 8, RT_STACK_LOCAL, {0, 0, 0, 0, 0}};
+  rt_tuning tuning = {8, 8, RT_STACK_LOCAL, rtb::W8_BRAID_PER_INSTANCE, {0, 0, 0, 0}};
   std::mutex mu;
   std::string last_error;
   std::atomic<uint64_t> rays{0}, launches{0}, scene_bytes{0};

@@ -456,7 +456,7 @@ void gather(uint32_t layout, const uint32_t* w, const uint32_t* rec, std::vector
 }  // namespace
 
 bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8Scene& out, std::string& err,
-                       int threads) {
+                       int threads, uint32_t per_instance) {
   (void)n_words;
   out = Wide8Scene{};
   const uint32_t count = w[0];
@@ -526,7 +526,7 @@ bool build_wide8_scene(uint32_t layout, const uint32_t* w, size_t n_words, Wide8
     out.inst[2 * i + 1] = tri_base[blas_of[i]];
   }
   out.blas_count = nb;
-  build_wide8_top_of(layout, w, out.nodes, out.inst, out.top_nodes, out.top_items, &out.top_depth);
+  build_wide8_top_of(layout, w, out.nodes, out.inst, out.top_nodes, out.top_items, &out.top_depth, per_instance);
   return true;
 }
 

@@ -115,8 +115,9 @@ bool instance_model(const uint32_t* rows, double* m);
 bool entry_object_box(const uint32_t* node, double* lo, double* hi);
 // The box of the eight corners of the object box [olo, ohi] under the affine map m (3 rows of 4).
 void entry_world_box(const double* m, const double* olo, const double* ohi, double* lo, double* hi);
+// `per_instance`: the top level's entries per instance (build_wide8_top_of).
 bool build_wide8_scene(uint32_t layout, const uint32_t* words, size_t n_words, Wide8Scene& out, std::string& err,
-                       int threads);
+                       int threads, uint32_t per_instance = W8_BRAID_PER_INSTANCE);
 // Checks a built layout (wide8_check.cpp): ranges, one leaf per triangle, every child box
 // enclosing its child in exact arithmetic, inverted empty slots, the recorded depth. info: nodes,
 // triangles, depth, distinct BLAS.

@@ -120,7 +120,8 @@ rt_status prepare_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>&
   RT_CUDA(ctx, cudaMemcpy(top.nodes.data(), d + scene->w8_nodes_at, top.nodes.size() * 4, cudaMemcpyDeviceToHost));
   if (!top.inst.empty())
     RT_CUDA(ctx, cudaMemcpy(top.inst.data(), d + scene->w8_inst_at, top.inst.size() * 4, cudaMemcpyDeviceToHost));
-  rtb::build_wide8_top_of(scene->layout, words.data(), top.nodes, top.inst, top.top_nodes, top.top_items, &top.top_depth);
+  rtb::build_wide8_top_of(scene->layout, words.data(), top.nodes, top.inst, top.top_nodes, top.top_items, &top.top_depth,
+                          ctx->tuning.wide8_entries);
   if (!rtb::check_wide8_top(scene->layout, words.data(), top, err)) top.top_nodes.clear();  // the packed top level
   return upload_top(ctx, scene, top.top_nodes, top.top_items);
 }
@@ -213,9 +214,11 @@ rt_status rt_ctx_set_tuning(rt_ctx* ctx, const rt_tuning* t) {
   for (uint32_t v : {t->fast_refill, t->wide8_refill})
     if (v > 32) return fail(ctx, RT_ERR_INVALID_ARG, "refill thresholds are 1-32 lanes");
   if (t->wide8_stack > RT_STACK_SHARED) return fail(ctx, RT_ERR_INVALID_ARG, "unknown stack placement %u", t->wide8_stack);
+  if (t->wide8_entries > 1024) return fail(ctx, RT_ERR_INVALID_ARG, "top-level entries per instance are 1-1024");
   if (t->fast_refill) next.fast_refill = t->fast_refill;
   if (t->wide8_refill) next.wide8_refill = t->wide8_refill;
   if (t->wide8_stack) next.wide8_stack = t->wide8_stack;
+  if (t->wide8_entries) next.wide8_entries = t->wide8_entries;
   ctx->tuning = next;
   return RT_OK;
 }
@@ -314,7 +317,7 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   rtb::Wide8Scene w8;
   std::string err;
   const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
-  if (!rtb::build_wide8_scene(scene->layout, words.data(), words.size(), w8, err, threads))
+  if (!rtb::build_wide8_scene(scene->layout, words.data(), words.size(), w8, err, threads, ctx->tuning.wide8_entries))
     return fail(ctx, RT_ERR_LAYOUT, "8-wide build: %s", err.c_str());
   // one allocation: nodes | triangles | instance table, each 16-byte aligned
   auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };

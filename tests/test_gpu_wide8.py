@@ -200,6 +200,54 @@ def test_packet_walk_over_a_top_level(engine, layout):
 
 
 @pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_wide8_rebraided_top_level(engine, layout):
+    """The 8-wide top level splits each instance's BLAS into world-space entries (up to 256 an
+    instance): over 400 rotated, scaled instances of four cluster meshes, some casting no shadow,
+    and random rays through their overlap, the per-ray walk finds the FP64 oracle's closest hits
+    and caster flags, and in every mode the same hits as over a top level of one entry per
+    instance (ids equal, t within the f64 band; flags equal) while entering far fewer."""
+    import torch
+    ms = S.multi_blas(n_blas=4, n_instances=400, tri_lo=2e3, tri_hi=2e4, half=300.0, config=11)
+    inst = ms.instances
+    inst.casts = (np.arange(len(inst)) % 5) != 2
+    w = product_words(layout, ms.meshes, inst)
+    assert w[1] != 0
+    rng = np.random.default_rng(21)
+    o = rng.uniform(-300.0, 300.0, (20_000, 3))
+    d = rng.normal(size=(20_000, 3))
+    rays = S.pack_rays(o, d / np.linalg.norm(d, axis=1, keepdims=True), 0.0, 1e30)
+    dev = torch.from_numpy(rays).cuda()
+    got, entered = {}, {}
+    try:
+        for entries in (1, 256):
+            engine.set_tuning(wide8_entries=entries)
+            scene = engine.upload(layout, w)
+            try:
+                scene.prepare("wide8")
+                for mode in (A.CLOSEST, A.ANY_SKY, A.ANY_CASTERS):
+                    got[entries, mode] = engine.trace(scene, dev, mode, "wide8").cpu().numpy().view(np.uint32)
+                c = engine.trace_counted(scene, dev[::8].contiguous(), A.CLOSEST, "wide8")
+                entered[entries] = c["instance_tests"] / c["rays"]
+            finally:
+                scene.release()
+    finally:
+        engine.set_tuning(wide8_entries=256)
+    ids = slice(1, 3) if layout == A.LAYOUT_REFLECTION else slice(1, 5)
+    a, b = got[1, A.CLOSEST], got[256, A.CLOSEST]
+    assert np.array_equal(a[:, ids], b[:, ids])
+    ta, tb = a[:, 0].view(np.float32), b[:, 0].view(np.float32)
+    assert np.all(np.abs(ta - tb) <= 2e-5 * np.abs(ta))
+    for mode in (A.ANY_SKY, A.ANY_CASTERS):
+        assert np.array_equal(got[1, mode], got[256, mode]), f"mode {mode}"
+    ref, ident = O.fp64_trace(w, rays, layout)
+    check_closest(layout, b, ref, ident, "re-braided top level")
+    ref_any, _ = O.fp64_trace(w, rays, layout, any_hit=True)
+    check_any(got[256, A.ANY_CASTERS].reshape(-1), rays, ref_any, "casters over the re-braided top level")
+    assert 0.2 < (ref[:, 0] > 0).mean() < 0.98
+    assert entered[256] < 0.7 * entered[1], entered
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
 def test_packet_walk_matches_the_per_ray_walk(engine, layout):
     """Per ray, the packet walk finds the per-ray walk's hit: ids equal, t within the f64
     band (the t of a winner the per-ray walk accepted in f32 may come back refined in f64), for
