@@ -710,10 +710,11 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
   L.phase = 0;
   const uint32_t count = ld(w, 0), top = ld(w, 1), root = ld(w, 2);
   const size_t top_base = LAYOUT == 0 ? top : (top & ~3u);
-  // the 8-wide top level's first nodes, staged once per block
-  __shared__ uint4 top_cache[5 * W8_TOP_CACHE];
+  // the 8-wide top level's first nodes, staged once per block (LAZY: the launches over scenes
+  // with a top level; a flat scene's launch keeps no shared memory, which leaves L1 more room)
+  __shared__ uint4 top_cache[5 * (LAZY ? W8_TOP_CACHE : 1)];
   const bool top8 = top != 0 && V.top != nullptr;
-  const uint32_t cached = top8 ? min(V.top_count, W8_TOP_CACHE) : 0u;
+  const uint32_t cached = LAZY && top8 ? min(V.top_count, W8_TOP_CACHE) : 0u;
   for (uint32_t i = threadIdx.x; i < 5 * cached; i += BLOCK) top_cache[i] = __ldg(V.top + i);
   __syncthreads();
   bool drained = false;
