@@ -35,15 +35,16 @@ constexpr uint32_t W8_STACK = 32;
 // levels deep stacks at most W8_SSTACK - 1 groups).
 constexpr uint32_t W8_SSTACK = 16;
 // Resident 128-thread blocks per SM the register allocation is sized for: the per-ray walk
-// (RT_W8_MIN_BLOCKS: 7, 72 registers) and the packet walk (RT_W8P_MIN_BLOCKS: 5, 96 registers).
-// The f64 resolution of uncertain candidates is out of line, so the hot loops fit these budgets
-// with a few bytes of spills. Measured on clusters-1M / clusters-4M GI rays against 4, 6 and 8
-// blocks: 7 is the fastest per-ray walk, 5 the fastest packet walk.
+// (RT_W8_MIN_BLOCKS: 7, 72 registers) and the packet walk (RT_W8P_MIN_BLOCKS: 7, 72 registers).
+// The f64 resolution of uncertain candidates is out of line, so the per-ray loop fits its budget
+// with a few bytes of spills (the packet walk with about 150). Measured on clusters-1M and
+// clusters-4M rays against 4 to 8 blocks, with neither walk holding shared memory: 7 is the
+// fastest for both.
 #ifndef RT_W8_MIN_BLOCKS
 #define RT_W8_MIN_BLOCKS 7
 #endif
 #ifndef RT_W8P_MIN_BLOCKS
-#define RT_W8P_MIN_BLOCKS 5
+#define RT_W8P_MIN_BLOCKS 7
 #endif
 
 // Opt-in device counters of the WIDE8 walk (diagnostics and the bytes-per-ray roofline).
@@ -802,12 +803,45 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
   }
 }
 
+// The packet walk's stacks, held in registers across the warp: entry i lives in lane i % 32, in
+// register i / 32 of that lane. The walk pushes and pops warp-uniform entries at a warp-uniform
+// depth, so a push is one predicated move and a pop one shuffle per register (no shared memory,
+// which leaves L1 its full size).
+template <int N>
+struct WarpStack {
+  uint32_t r[(N + 31) / 32];
+  RT_DEV void put(uint32_t at, uint32_t v) {
+#pragma unroll
+    for (int k = 0; k < (N + 31) / 32; ++k)
+      if (at == (uint32_t)(threadIdx.x & 31) + 32u * k) r[k] = v;
+  }
+  RT_DEV uint32_t get(uint32_t at) const {
+    uint32_t v = 0;
+#pragma unroll
+    for (int k = 0; k < (N + 31) / 32; ++k) {
+      const uint32_t x = __shfl_sync(0xffffffffu, r[k], at & 31u);
+      if ((at >> 5) == (uint32_t)k) v = x;
+    }
+    return v;
+  }
+};
+struct WarpGroupStack {  // W8_STACK (32) node-group entries: (first child, pending bits | inner mask << 8)
+  uint32_t base, bits;
+  RT_DEV void put(uint32_t at, uint2 e) {
+    if (at == (threadIdx.x & 31)) base = e.x, bits = e.y;
+  }
+  RT_DEV uint2 get(uint32_t at) const {
+    return make_uint2(__shfl_sync(0xffffffffu, base, at), __shfl_sync(0xffffffffu, bits, at));
+  }
+};
+static_assert(W8_STACK == 32, "WarpGroupStack holds one entry a lane");
+
 // One top-level node of the packet walk: each live lane computes its four slab entries against its
 // own bound (the per-ray walk's, from its best hit); a child is visited when any lane meets it,
-// nearest (over the lanes' entries) first. Lane 0 pushes onto the warp's top stack; every lane
-// returns the stack's new depth.
-RT_DEV uint32_t w8_packet_top(const uint32_t* __restrict__ w, size_t n, const W8Lane& L, bool live, uint32_t* tstack,
-                              uint32_t sp, DevStatus* st) {
+// nearest (over the lanes' entries) first, pushed onto the warp's top stack. Every lane returns
+// the stack's new depth.
+RT_DEV uint32_t w8_packet_top(const uint32_t* __restrict__ w, size_t n, const W8Lane& L, bool live,
+                              WarpStack<STACK>& tstack, uint32_t sp, DevStatus* st) {
   uint32_t key[4], ids[4];
   const W8Best& b = L.best;
   const float bound = b.hit ? b.t + 2.0f * b.band + 2.0f * W8_TIE * b.t : b.t;
@@ -846,13 +880,12 @@ RT_DEV uint32_t w8_packet_top(const uint32_t* __restrict__ w, size_t n, const W8
   for (int c = 3; c >= 0; --c) {  // far to near: the nearest is popped first
     if (key[c] == 0xffffffffu) continue;
     if (sp < STACK) {
-      if (lane == 0) tstack[sp] = ids[c];
+      tstack.put(sp, ids[c]);
       ++sp;
     } else if (lane == 0) {
       atomicAdd(&st->stack_drops, 1ull);
     }
   }
-  __syncwarp();
   return sp;
 }
 
@@ -861,18 +894,16 @@ RT_DEV uint32_t w8_packet_top(const uint32_t* __restrict__ w, size_t n, const W8
 // 8-wide BLAS. A node's child is visited when any lane's ray meets its box, in the first entering
 // lane's octant order (top-level nodes: nearest entry over the lanes first), so every lane reads
 // the same node (one broadcast load) and no lane diverges on the walk; the traversal stacks are
-// the warp's, in shared memory. Each lane still tests its own ray against every visited node's
-// boxes (its own hits and closest-hit bound), enters only the instances whose world box its ray
-// meets, and tests the triangles of the leaves its ray meets. WIDE8's results do not depend on
+// the warp's, in registers (WarpStack). Each lane still tests its own ray against every visited
+// node's boxes (its own hits and closest-hit bound), enters only the instances whose world box its
+// ray meets, and tests the triangles of the leaves its ray meets. WIDE8's results do not depend on
 // the visit order (conservative boxes, ties resolved in f64 on (t, instance, triangle)), so each
 // ray gets the hit the per-ray walk finds.
 template <uint32_t LAYOUT, int AM, int BLOCK, class Src>
 __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const uint32_t* __restrict__ w, W8View V, const Src src,
                                                            unsigned int* __restrict__ counter, uint32_t n, DevStatus* st) {
-  __shared__ uint2 warp_stack[BLOCK / 32][W8_STACK];
-  __shared__ uint32_t warp_top[BLOCK / 32][STACK];
-  uint2* stack = warp_stack[threadIdx.x >> 5];
-  uint32_t* tstack = warp_top[threadIdx.x >> 5];
+  WarpGroupStack stack;
+  WarpStack<STACK> tstack;
   const int lane = threadIdx.x & 31;
   const uint32_t count = ld(w, 0), top = ld(w, 1), root = ld(w, 2);
   const size_t top_base = LAYOUT == 0 ? top : (top & ~3u);
@@ -894,8 +925,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
     }
     uint32_t flat = 0, tsp = 0;
     if (top != 0 && count != 0) {
-      if (lane == 0) tstack[0] = root;
-      __syncwarp();
+      tstack.put(0, root);
       tsp = 1;
     }
     while (__any_sync(0xffffffffu, live)) {
@@ -905,8 +935,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
         i = flat++;
       } else {
         if (tsp == 0) break;
-        const uint32_t item = tstack[--tsp];
-        __syncwarp();  // every lane has read the entry before lane 0 may overwrite it
+        const uint32_t item = tstack.get(--tsp);
         if (!(item & LEAF)) {
           tsp = w8_packet_top(w, top_base + (size_t)item * 32, L, live, tstack, tsp, st);
           continue;
@@ -923,7 +952,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
       for (;;) {
         if (node == EMPTY) {  // the warp's next node (uniform)
           while (g_bits == 0 && sp > 0) {
-            const uint2 e = stack[--sp];
+            const uint2 e = stack.get(--sp);
             g_base = e.x, g_bits = e.y & 0xffu, g_imask = e.y >> 8;
           }
           if (g_bits == 0) break;
@@ -958,8 +987,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
         if (inner) {
           if (g_bits) {
             if (sp < W8_STACK) {
-              if (lane == 0) stack[sp] = make_uint2(g_base, g_bits | g_imask << 8);
-              __syncwarp();
+              stack.put(sp, make_uint2(g_base, g_bits | g_imask << 8));
               ++sp;
             } else if (lane == 0) {
               atomicAdd(&st->stack_drops, 1ull);
