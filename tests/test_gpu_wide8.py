@@ -278,6 +278,82 @@ def test_packet_walk_matches_the_per_ray_walk(engine, layout):
         scene.release()
 
 
+def _narrow_batches(mesh, n_packets=600, seed=5):
+    """Packets of 32 consecutive rays that share a direction octant within a narrow cone, with
+    origins and directions spread in the ways that stress the packet walk's shared traversal:
+    scattered origins, rays that graze edges and vertices, zero and sub-clamp components."""
+    rng = np.random.default_rng(seed)
+    p = mesh.positions.astype(np.float64)
+    tri = mesh.indices.reshape(-1, 3)
+    out = []
+    # (1) parallel rays, as toward a directional light, from points on random triangles (origins
+    # spread over the scene, or within one cluster's neighbourhood after a sort by origin)
+    k = rng.integers(0, len(tri), 32 * n_packets)
+    b = rng.dirichlet((1.0, 1.0, 1.0), 32 * n_packets)
+    on = (p[tri[k, 0]] * b[:, :1] + p[tri[k, 1]] * b[:, 1:2] + p[tri[k, 2]] * b[:, 2:3])
+    sun = np.array([0.3, 0.8, 0.2]) / np.linalg.norm([0.3, 0.8, 0.2])
+    o = on + 1e-3 * sun
+    out.append(S.pack_rays(o, np.tile(sun, (len(o), 1)), 0.0, 1e30))
+    order = np.lexsort((o[:, 2], np.floor(o[:, 1] / 8.0), np.floor(o[:, 0] / 8.0)))
+    out.append(S.pack_rays(o[order], np.tile(-sun, (len(o), 1)), 0.0, 1e30))
+    # (2) one origin, each packet aimed at one triangle: rays through its vertices and through
+    # points 1e-7 .. 1e-3 (relative) off its edges, inside and outside
+    eye = np.array([0.0, 0.0, -250.0])
+    k = np.repeat(rng.integers(0, len(tri), n_packets), 32)
+    e = rng.integers(0, 3, len(k))
+    t = rng.uniform(0.0, 1.0, len(k))
+    t[::8] = 0.0  # a vertex
+    v0, v1, v2 = p[tri[k, e]], p[tri[k, (e + 1) % 3]], p[tri[k, (e + 2) % 3]]
+    on_edge = v0 * (1 - t)[:, None] + v1 * t[:, None]
+    inward = v2 - on_edge
+    off = rng.choice([-1.0, 1.0], len(k)) * 10.0 ** rng.uniform(-7, -3, len(k))
+    target = on_edge + inward * off[:, None]
+    d = target - eye
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    out.append(S.pack_rays(np.tile(eye, (len(d), 1)), d, 0.0, 1e30))
+    # (3) directions with a zero (+0 or -0) or tiny (below the 1e-30 clamp) component, mixed in a
+    # packet, from a scattered line of origins across the scene
+    n = 32 * n_packets
+    o = np.stack([rng.uniform(-150, 150, n), rng.uniform(-120, 120, n), np.full(n, -260.0)], axis=1)
+    d = np.tile(np.array([0.05, 0.0, 1.0]), (n, 1))
+    d[:, 1] = rng.choice([0.0, -0.0, 1e-35, -1e-35, 1e-20], n)
+    d[:, 0] = rng.choice([0.05, 0.0, -0.0], n) * (np.arange(n) // 32 % 2)
+    out.append(S.pack_rays(o, d / np.linalg.norm(d, axis=1, keepdims=True), 0.0, 1e30))
+    return out
+
+
+@pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
+def test_packet_walk_on_narrow_packets_matches_the_per_ray_walk(engine, layout):
+    """On parallel rays from scattered origins, narrow cones aimed at vertices and within 1e-7 of
+    edges, and directions with zero or sub-clamp components, the packet walk returns the per-ray
+    walk's hits (ids equal, t within the f64 band; any-hit flags equal) and the FP64 oracle's hit
+    ids."""
+    import torch
+    mesh, _ = H.small_clusters(60_000, 64, 64)
+    w = product_words(layout, [mesh], S.identity_instances(1))
+    scene = engine.upload(layout, w)
+    ids = slice(1, 3) if layout == A.LAYOUT_REFLECTION else slice(1, 5)
+    try:
+        scene.prepare("wide8")
+        for j, batch in enumerate(_narrow_batches(mesh)):
+            d = torch.from_numpy(batch).cuda()
+            a = engine.trace(scene, d, A.CLOSEST, "wide8").cpu().numpy().view(np.uint32)
+            b = engine.trace(scene, d, A.CLOSEST, "wide8p").cpu().numpy().view(np.uint32)
+            assert np.array_equal(a[:, ids], b[:, ids]), f"batch {j}: {(a[:, ids] != b[:, ids]).any(1).sum()} rays differ"
+            ta, tb = a[:, 0].view(np.float32), b[:, 0].view(np.float32)
+            assert np.all(np.abs(ta - tb) <= 2e-5 * np.abs(ta)), f"batch {j}"
+            for mode in (A.ANY_SKY, A.ANY_CASTERS):
+                fa = engine.trace(scene, d, mode, "wide8").cpu().numpy()
+                fb = engine.trace(scene, d, mode, "wide8p").cpu().numpy()
+                assert np.array_equal(fa, fb), f"batch {j} mode {mode}: {(fa != fb).sum()} flags differ"
+            sub = slice(0, 32 * 96)
+            ref, ident = O.fp64_trace(w, batch[sub], layout)
+            check_closest(layout, b[sub], ref, ident, f"packet walk, narrow batch {j}")
+            assert (b[:, 1] != (A.MISS if layout == A.LAYOUT_GI else 0)).any()
+    finally:
+        scene.release()
+
+
 def test_wide8_far_small_triangles_near_edges(engine, w8kernel):
     """Isolated small triangles (0.05 units) 200 units down the view axis and 50 units to its
     side, rays aimed within 1e-6 to 1e-3 of an edge, inside and outside. The shear's rounding grows
