@@ -151,6 +151,18 @@ rt_status rt_scene_update_records(rt_ctx* ctx, rt_scene* scene, const uint32_t* 
 /* Builds the derived layout a kernel needs (RT_KERNEL_WIDE8: the compressed 8-wide BVH over the
  * scene's triangles, built on the host threads and uploaded). PLAIN and FAST need nothing. */
 rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel);
+/* Chooses the WIDE8 top level's entries per instance for this scene by measurement: for each
+ * budget (NULL / 0 budgets: 1, 4, 16, 64, 256; each 1-1024), rebuilds only the 8-wide top level
+ * and times a WIDE8 pass over `probe` seeded incoherent rays in the scene's world box (0:
+ * 65,536; half closest-hit with uniform directions, half any-hit toward uniform points of the
+ * box), then keeps the fastest, which the scene's later rt_scene_prepare calls also use, and
+ * reports it in *chosen (0 for a scene without a top level, which is left as it is). Few large
+ * instances favour 1 (each instance entered at its BLAS root); many small, deeply overlapping
+ * ones favour more. Needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first; synchronous. No
+ * counterpart in the reference, whose top level is the packed BVH4 over instance boxes
+ * (src/instance_bvh.rs:162-460). */
+rt_status rt_scene_tune_top(rt_ctx* ctx, rt_scene* scene, const uint32_t* budgets, uint32_t n_budgets,
+                            uint32_t probe, uint32_t* chosen);
 /* Levels of the deepest 8-wide BLAS (after rt_scene_prepare for WIDE8, else RT_ERR_UNSUPPORTED):
  * RT_STACK_SHARED needs at most 16. */
 rt_status rt_scene_wide8_depth(const rt_scene* scene, uint32_t* depth);
@@ -303,7 +315,8 @@ typedef struct rt_server_desc {
   uint64_t hbm_budget;  /* device bytes for scenes + launch slots */
   uint32_t launch_rays; /* rays a launch slot holds (a request larger than this spans slots) */
   uint32_t slots;       /* launch slots in flight at once (1-64) */
-  rt_kernel kernel;     /* RT_KERNEL_PLAIN, RT_KERNEL_FAST or RT_KERNEL_WIDE8 (scenes prepared on add) */
+  rt_kernel kernel;     /* RT_KERNEL_PLAIN, RT_KERNEL_FAST or RT_KERNEL_WIDE8 (scenes prepared on add,
+                         * and a scene with a top level gets its entries tuned by rt_scene_tune_top) */
 } rt_server_desc;
 typedef struct rt_server_stats {
   uint64_t requests;    /* finished since the last reset */

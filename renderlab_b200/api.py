@@ -102,7 +102,7 @@ EXPORTS = ("rt_abi_version", "rt_ctx_create", "rt_ctx_destroy", "rt_get_last_err
            "rt_selftest", "rt_scene_upload", "rt_scene_update_records", "rt_scene_release",
            "rt_scene_device_bytes", "rt_scene_validate", "rt_scene_prepare", "rt_trace", "rt_trace_ex", "rt_trace_host", "rt_trace_host_batches", "rt_ctx_reserve", "rt_trace_counted", "rt_order_rays",
            "rt_trace_batches", "rt_plan_create", "rt_plan_launch", "rt_plan_info", "rt_plan_destroy",
-           "rt_scene_refit", "rt_scene_read_words", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_trace_gi_lights", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
+           "rt_scene_refit", "rt_scene_read_words", "rt_scene_tune_top", "rt_gi_cell_rays", "rt_trace_gi_cells", "rt_trace_gi_lights", "rt_server_create", "rt_server_add_scene", "rt_server_remove_scene", "rt_server_submit",
            "rt_server_wait", "rt_server_get_stats", "rt_server_fail_next", "rt_server_destroy",
            "rt_trace_static", "rt_trace_static_stack_drops", "rt_read_bandwidth", "rt_scene_wide8_depth", "rt_wide8_check", "rt_object_box", "rt_move_instances_host",
            "rt_scene_move_instances", "rt_blas_build", "rt_blas_build_device", "rt_blas_info", "rt_blas_nodes", "rt_blas_indices", "rt_blas_refit",
@@ -138,6 +138,7 @@ def lib() -> ctypes.CDLL:
     L.rt_scene_release.argtypes = [_vp, _vp]
     L.rt_scene_prepare.argtypes = [_vp, _vp, ctypes.c_int]
     L.rt_scene_wide8_depth.argtypes = [_vp, _u32p]
+    L.rt_scene_tune_top.argtypes = [_vp, _vp, _u32p, ctypes.c_uint32, ctypes.c_uint32, _u32p]
     L.rt_wide8_check.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, _u32p, ctypes.c_char_p, ctypes.c_size_t]
     L.rt_object_box.argtypes = [ctypes.c_int, _vp, _f32p, _u32p, ctypes.c_uint32, _f32p]
     L.rt_move_instances_host.argtypes = [ctypes.c_int, _u32p, ctypes.c_size_t, ctypes.POINTER(RtInstance),
@@ -455,6 +456,16 @@ class Scene:
         s = stream
         self.engine._check(lib().rt_scene_move_instances(self.engine.ctx, self.handle, arr, n, _np_ptr(boxes, _f32p),
                                                          len(boxes), s))
+
+    def tune_top(self, budgets=None, probe: int = 0) -> int:
+        """rt_scene_tune_top: measures the WIDE8 top level's entries per instance over a probe of
+        incoherent closest- and any-hit rays (after prepare("wide8")), keeps the fastest and
+        returns it (0: the scene has no top level)."""
+        b = None if budgets is None else np.ascontiguousarray(budgets, np.uint32)
+        out = ctypes.c_uint32()
+        self.engine._check(lib().rt_scene_tune_top(self.engine.ctx, self.handle, _np_ptr(b, _u32p) if b is not None else None,
+                                                   0 if b is None else len(b), probe, ctypes.byref(out)))
+        return int(out.value)
 
     def wide8_depth(self) -> int:
         """Levels of the deepest 8-wide BLAS (after prepare("wide8")); the shared stack takes 16."""

@@ -44,6 +44,8 @@ struct rt_scene {
   size_t w8_top_bytes = 0, w8_top_items_at = 0;
   uint32_t w8_top_nodes = 0;
   bool w8_top_valid = false;
+  uint32_t w8_entries = 0;  // the top level's entries per instance (rt_scene_tune_top); 0: the context's
+
   std::map<uint32_t, RefitLevels> refit;  // by the BLAS's node base word
   // rt_scene_move_instances: staging for the moved instances and mesh boxes, and the top level's
   // nodes grouped by height (deepest last), kept until a rebuild changes the tree.

@@ -109,21 +109,40 @@ rt_status upload_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& 
   return RT_OK;
 }
 
-// Rebuilds only the 8-wide top level, from the scene's current records and its built 8-wide
-// BLAS nodes and instance table (read back from the device).
-rt_status prepare_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& words) {
-  rtb::Wide8Scene top;
-  std::string err;
+// The top level's entries per instance for this scene: its tuned budget, else the context's.
+uint32_t entries_of(const rt_ctx* ctx, const rt_scene* scene) {
+  return scene->w8_entries ? scene->w8_entries : ctx->tuning.wide8_entries;
+}
+
+// Host copies of the scene's built 8-wide BLAS nodes and instance table (read back from the device).
+rt_status read_wide8_blas(rt_ctx* ctx, const rt_scene* scene, uint32_t instances, rtb::Wide8Scene& top) {
   top.nodes.resize(scene->w8_tris_at - scene->w8_nodes_at);
-  top.inst.resize(2 * (size_t)words[0]);
+  top.inst.resize(2 * (size_t)instances);
   const uint32_t* d = static_cast<const uint32_t*>(scene->d_wide8);
   RT_CUDA(ctx, cudaMemcpy(top.nodes.data(), d + scene->w8_nodes_at, top.nodes.size() * 4, cudaMemcpyDeviceToHost));
   if (!top.inst.empty())
     RT_CUDA(ctx, cudaMemcpy(top.inst.data(), d + scene->w8_inst_at, top.inst.size() * 4, cudaMemcpyDeviceToHost));
+  return RT_OK;
+}
+
+// Builds and uploads the 8-wide top level with `entries` leaves per instance over `top`'s BLAS
+// nodes and instance table (the packed top level when the build or its check fails).
+rt_status rebuild_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& words, rtb::Wide8Scene& top,
+                      uint32_t entries) {
+  std::string err;
   rtb::build_wide8_top_of(scene->layout, words.data(), top.nodes, top.inst, top.top_nodes, top.top_items, &top.top_depth,
-                          ctx->tuning.wide8_entries);
+                          entries);
   if (!rtb::check_wide8_top(scene->layout, words.data(), top, err)) top.top_nodes.clear();  // the packed top level
   return upload_top(ctx, scene, top.top_nodes, top.top_items);
+}
+
+// Rebuilds only the 8-wide top level, from the scene's current records and its built 8-wide
+// BLAS nodes and instance table.
+rt_status prepare_top(rt_ctx* ctx, rt_scene* scene, const std::vector<uint32_t>& words) {
+  rtb::Wide8Scene top;
+  rt_status s = read_wide8_blas(ctx, scene, words[0], top);
+  if (s != RT_OK) return s;
+  return rebuild_top(ctx, scene, words, top, entries_of(ctx, scene));
 }
 
 // Frees the scene's derived 8-wide layout (its BLASes, instance table and top level): WIDE8 then
@@ -317,7 +336,7 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel) {
   rtb::Wide8Scene w8;
   std::string err;
   const int threads = (int)std::max(1u, std::thread::hardware_concurrency());
-  if (!rtb::build_wide8_scene(scene->layout, words.data(), words.size(), w8, err, threads, ctx->tuning.wide8_entries))
+  if (!rtb::build_wide8_scene(scene->layout, words.data(), words.size(), w8, err, threads, entries_of(ctx, scene)))
     return fail(ctx, RT_ERR_LAYOUT, "8-wide build: %s", err.c_str());
   // one allocation: nodes | triangles | instance table, each 16-byte aligned
   auto up4 = [](size_t x) { return (x + 3) & ~(size_t)3; };
@@ -366,6 +385,126 @@ rt_status rt_scene_wide8_depth(const rt_scene* scene, uint32_t* depth) {
   if (!scene->d_wide8) return RT_ERR_UNSUPPORTED;
   *depth = scene->w8_depth;
   return RT_OK;
+}
+
+namespace {
+// Seeded uniform floats for the top-level probe (splitmix64, top 24 bits).
+struct ProbeRng {
+  uint64_t s;
+  float next() {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return (float)((z ^ (z >> 31)) >> 40) * (1.0f / 16777216.0f);
+  }
+};
+
+// The probe of rt_scene_tune_top: n incoherent rays over the scene's world box, the first half
+// closest-hit queries (origins uniform in the box, directions uniform on the sphere), the rest
+// any-hit queries toward a uniform point of the box, stopping short of it.
+std::vector<float> probe_rays(const rtb::Aabb& box, uint32_t n) {
+  std::vector<float> r(8 * (size_t)n);
+  ProbeRng g{0x70B5EEDull};
+  auto point = [&](float* p) {
+    for (int a = 0; a < 3; ++a) p[a] = box.lo[a] + (box.hi[a] - box.lo[a]) * g.next();
+  };
+  for (uint32_t i = 0; i < n; ++i) {
+    float* x = r.data() + 8 * (size_t)i;
+    point(x);
+    x[3] = 0.0f;
+    float d[3], len = 0.0f;
+    if (i < n / 2) {
+      const float z = 2.0f * g.next() - 1.0f, phi = 6.2831853f * g.next(), s = std::sqrt(std::max(0.0f, 1.0f - z * z));
+      d[0] = s * std::cos(phi), d[1] = s * std::sin(phi), d[2] = z;
+      x[7] = 1e30f;
+    } else {
+      float q[3];
+      point(q);
+      for (int a = 0; a < 3; ++a) d[a] = q[a] - x[a];
+      len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+      if (!(len > 1e-3f)) d[0] = 1.0f, d[1] = d[2] = 0.0f, len = 1e-3f;
+      else for (int a = 0; a < 3; ++a) d[a] /= len;
+      x[7] = len * (1.0f - 1e-4f);
+    }
+    x[4] = d[0], x[5] = d[1], x[6] = d[2];
+  }
+  return r;
+}
+}  // namespace
+
+rt_status rt_scene_tune_top(rt_ctx* ctx, rt_scene* scene, const uint32_t* budgets, uint32_t n_budgets,
+                            uint32_t probe, uint32_t* chosen) {
+  if (!ctx || !scene) return fail(ctx, RT_ERR_INVALID_ARG, "null argument");
+  if (n_budgets > 16 || (n_budgets && !budgets)) return fail(ctx, RT_ERR_INVALID_ARG, "0-16 budgets");
+  for (uint32_t k = 0; k < n_budgets; ++k)
+    if (budgets[k] == 0 || budgets[k] > 1024) return fail(ctx, RT_ERR_INVALID_ARG, "entries per instance are 1-1024");
+  if (!scene->d_wide8) return fail(ctx, RT_ERR_UNSUPPORTED, "rt_scene_tune_top needs rt_scene_prepare(scene, RT_KERNEL_WIDE8)");
+  if (chosen) *chosen = 0;
+  if (scene->info.top == 0 || scene->info.instances < 2) return RT_OK;  // no top level to tune
+  static const uint32_t kDefault[] = {1, 4, 16, 64, 256};
+  if (n_budgets == 0) budgets = kDefault, n_budgets = 5;
+  const uint32_t n = std::max<uint32_t>(64, std::min<uint32_t>(probe ? probe : 1u << 16, 1u << 22));
+  rtb::Aabb box = scene->info.world;
+  for (int a = 0; a < 3; ++a)
+    if (!std::isfinite(box.lo[a]) || !std::isfinite(box.hi[a]) || !(box.hi[a] >= box.lo[a]))
+      return fail(ctx, RT_ERR_LAYOUT, "the scene has no finite world box to probe");
+  std::vector<uint32_t> words(scene->n_words);
+  RT_CUDA(ctx, cudaSetDevice(ctx->device));
+  RT_CUDA(ctx, cudaMemcpy(words.data(), scene->d_words, scene->n_words * 4, cudaMemcpyDeviceToHost));
+  rtb::Wide8Scene top;
+  rt_status s = read_wide8_blas(ctx, scene, words[0], top);
+  if (s != RT_OK) return s;
+  const std::vector<float> rays = probe_rays(box, n);
+  const size_t hit_words = scene->layout == 0 ? 10 : 5;
+  void *d_rays = nullptr, *d_hits = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto cleanup = [&]() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (stream) cudaStreamDestroy(stream);
+    cudaFree(d_rays);
+    cudaFree(d_hits);
+  };
+  if (cudaMalloc(&d_rays, rays.size() * 4) != cudaSuccess || cudaMalloc(&d_hits, hit_words * 4 * (size_t)n) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking) != cudaSuccess || cudaEventCreate(&e0) != cudaSuccess ||
+      cudaEventCreate(&e1) != cudaSuccess || cudaMemcpy(d_rays, rays.data(), rays.size() * 4, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaGetLastError();
+    cleanup();
+    return fail(ctx, RT_ERR_OOM, "top-level probe buffers for %u rays", n);
+  }
+  const rt_ray* pr = static_cast<const rt_ray*>(d_rays);
+  const uint32_t half = n / 2;
+  // one pass of the probe: the closest-hit half, then the any-hit half, WIDE8 on the probe's stream
+  auto pass = [&]() -> rt_status {
+    rt_status t = dispatch(ctx, scene, RT_CLOSEST, RT_KERNEL_WIDE8, pr, nullptr, d_hits, half, stream);
+    if (t == RT_OK) t = dispatch(ctx, scene, RT_ANY_CASTERS, RT_KERNEL_WIDE8, pr + half, nullptr, d_hits, n - half, stream);
+    return t;
+  };
+  uint32_t best = 0;
+  float best_ms = 0.0f;
+  for (uint32_t k = 0; k < n_budgets && s == RT_OK; ++k) {
+    s = rebuild_top(ctx, scene, words, top, budgets[k]);
+    if (s != RT_OK) break;
+    float ms = 0.0f;
+    for (int rep = 0; rep < 3 && s == RT_OK; ++rep) {  // a warm-up pass, then the faster of two timed ones
+      cudaEventRecord(e0, stream);
+      s = pass();
+      cudaEventRecord(e1, stream);
+      if (s != RT_OK) break;
+      if (cudaEventSynchronize(e1) != cudaSuccess) s = fail(ctx, RT_ERR_CUDA, "top-level probe: %s", cudaGetErrorString(cudaGetLastError()));
+      float t = 0.0f;
+      cudaEventElapsedTime(&t, e0, e1);
+      if (rep == 1 || (rep == 2 && t < ms)) ms = t;
+    }
+    if (s == RT_OK && (best == 0 || ms < best_ms)) best = budgets[k], best_ms = ms;
+  }
+  cleanup();
+  if (s != RT_OK) return s;
+  scene->w8_entries = best;
+  if (best != budgets[n_budgets - 1]) s = rebuild_top(ctx, scene, words, top, best);
+  if (s == RT_OK && chosen) *chosen = best;
+  return s;
 }
 
 rt_status rt_scene_release(rt_ctx* ctx, rt_scene* scene) {

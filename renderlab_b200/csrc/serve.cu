@@ -287,7 +287,10 @@ rt_status rt_server_add_scene(rt_server* srv, rt_layout layout, const uint32_t* 
   rt_scene* scene = nullptr;
   rt_status st = rt_scene_upload(ctx, layout, words, n_words, &scene);
   if (st != RT_OK) return st;
-  if (srv->desc.kernel >= RT_KERNEL_WIDE8 && (st = rt_scene_prepare(ctx, scene, RT_KERNEL_WIDE8)) != RT_OK) {
+  // WIDE8: the derived layout, and the top level's entries per instance measured for this scene
+  if (srv->desc.kernel >= RT_KERNEL_WIDE8 &&
+      ((st = rt_scene_prepare(ctx, scene, RT_KERNEL_WIDE8)) != RT_OK ||
+       (st = rt_scene_tune_top(ctx, scene, nullptr, 0, 0, nullptr)) != RT_OK)) {
     rt_scene_release(ctx, scene);
     return st;
   }

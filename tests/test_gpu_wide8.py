@@ -247,6 +247,60 @@ def test_wide8_rebraided_top_level(engine, layout):
     assert entered[256] < 0.7 * entered[1], entered
 
 
+def test_tune_top_keeps_a_measured_budget_and_every_result(engine):
+    """rt_scene_tune_top rebuilds only the 8-wide top level per candidate budget, keeps the fastest
+    on its probe (one of the candidates, kept by a later prepare after records change), and the
+    walk over the chosen top level finds the FP64 oracle's hits and caster flags. A flat scene has
+    nothing to tune (0); an unprepared scene and out-of-range budgets are refused."""
+    import torch
+    layout = A.LAYOUT_REFLECTION
+    ms = S.multi_blas(n_blas=4, n_instances=300, tri_lo=2e3, tri_hi=2e4, half=300.0, config=12)
+    inst = ms.instances
+    inst.casts = (np.arange(len(inst)) % 4) != 1
+    w = product_words(layout, ms.meshes, inst)
+    rng = np.random.default_rng(31)
+    o = rng.uniform(-300.0, 300.0, (12_000, 3))
+    d = rng.normal(size=(12_000, 3))
+    rays = S.pack_rays(o, d / np.linalg.norm(d, axis=1, keepdims=True), 0.0, 1e30)
+    dev = torch.from_numpy(rays).cuda()
+    scene = engine.upload(layout, w)
+    try:
+        with pytest.raises(A.RtError):
+            scene.tune_top()  # not prepared
+        scene.prepare("wide8")
+        for bad in ([0], [2000]):
+            with pytest.raises(A.RtError):
+                scene.tune_top(bad)
+        chosen = scene.tune_top([1, 16, 256], probe=8192)
+        assert chosen in (1, 16, 256)
+        got = engine.trace(scene, dev, A.CLOSEST, "wide8").cpu().numpy().view(np.uint32)
+        flags = engine.trace(scene, dev, A.ANY_CASTERS, "wide8").cpu().numpy()
+        ref, ident = O.fp64_trace(w, rays, layout)
+        check_closest(layout, got, ref, ident, f"top level tuned to {chosen} entries an instance")
+        ref_any, _ = O.fp64_trace(w, rays, layout, any_hit=True)
+        check_any(flags.reshape(-1), rays, ref_any, "casters over the tuned top level")
+        # default candidates; the choice survives a records rewrite and re-prepare
+        chosen = scene.tune_top()
+        assert chosen in (1, 4, 16, 64, 256)
+        before = engine.trace_counted(scene, dev[::4].contiguous(), A.CLOSEST, "wide8")
+        scene.update_records(w)
+        scene.prepare("wide8")
+        after = engine.trace_counted(scene, dev[::4].contiguous(), A.CLOSEST, "wide8")
+        assert (before["top_nodes"], before["instance_tests"]) == (after["top_nodes"], after["instance_tests"])
+        again = engine.trace(scene, dev, A.CLOSEST, "wide8").cpu().numpy().view(np.uint32)
+        ids = slice(1, 3)
+        assert np.array_equal(again[:, ids], got[:, ids])
+    finally:
+        scene.release()
+    mesh, _ = H.small_clusters(20_000, 16, 16)
+    flat = engine.upload(layout, product_words(layout, [mesh], S.identity_instances(1)))
+    try:
+        flat.prepare("wide8")
+        assert flat.tune_top() == 0
+    finally:
+        flat.release()
+
+
 @pytest.mark.parametrize("layout", [A.LAYOUT_GI, A.LAYOUT_REFLECTION])
 def test_packet_walk_matches_the_per_ray_walk(engine, layout):
     """Per ray, the packet walk finds the per-ray walk's hit: ids equal, t within the f64
