@@ -84,7 +84,7 @@ struct CellRays {
   uint32_t rotate;
   void* out;
 };
-template <class Lane>
+template <bool CS = false, class Lane>  // CS: no ray is read (the ray is made here)
 RT_DEV Ray fetch(const CellRays& s, uint32_t id, Lane& L) {
   L.ray_id = id;
   L.entry = 0;
@@ -155,7 +155,7 @@ RT_DEV Ray gi_light_ray(const LightRays& s, uint32_t i) {
   gi_light_direction(light, q, d, dist);
   return Ray{o, 0.0f, d, gi_light_affects(light, n, d, dist) ? dist : -1.0f};
 }
-template <class Lane>
+template <bool CS = false, class Lane>  // CS: no ray is read (the ray is made here)
 RT_DEV Ray fetch(const LightRays& s, uint32_t id, Lane& L) {
   L.ray_id = id;
   L.entry = 0;

@@ -76,6 +76,16 @@ RT_DEV Ray load_ray(const float4* __restrict__ rays, uint32_t i) {
   float4 a = __ldg(rays + 2 * (size_t)i), b = __ldg(rays + 2 * (size_t)i + 1);
   return Ray{{a.x, a.y, a.z}, a.w, {b.x, b.y, b.z}, b.w};
 }
+// The streaming form (ld.global.cs: evict first from L1 and L2): a walk reads each ray once, and
+// a launch's ray stream (32 bytes a ray, hundreds of MB) should not push the scene out of L2.
+RT_DEV Ray load_ray_cs(const float4* __restrict__ rays, uint32_t i) {
+  float4 a = __ldcs(rays + 2 * (size_t)i), b = __ldcs(rays + 2 * (size_t)i + 1);
+  return Ray{{a.x, a.y, a.z}, a.w, {b.x, b.y, b.z}, b.w};
+}
+template <bool CS>
+RT_DEV Ray load_ray_as(const float4* __restrict__ rays, uint32_t i) {
+  return CS ? load_ray_cs(rays, i) : load_ray(rays, i);
+}
 
 // One ray batch of a many-batch launch, as the device reads it (32 bytes).
 struct BatchEntry {
@@ -109,13 +119,14 @@ RT_DEV bool any_of(const Lane& L) {
   return AM == 2 ? L.any : AM == 1;
 }
 
-template <class Lane>
+// CS: the ray is read in the streaming form (load_ray_cs).
+template <bool CS = false, class Lane>
 RT_DEV Ray fetch(const OneBatch& s, uint32_t id, Lane& L) {
   L.ray_id = s.order ? __ldg(s.order + id) : id;
   L.entry = 0;
-  return load_ray(s.rays, L.ray_id);
+  return load_ray_as<CS>(s.rays, L.ray_id);
 }
-template <class Lane>
+template <bool CS = false, class Lane>
 RT_DEV Ray fetch(const ManyBatches& s, uint32_t id, Lane& L) {
   const uint32_t g = s.order ? __ldg(s.order + id) : id;
   uint32_t lo = 0, hi = s.entries;  // the last entry whose first ray is at or before g
@@ -128,7 +139,7 @@ RT_DEV Ray fetch(const ManyBatches& s, uint32_t id, Lane& L) {
   L.entry = lo;
   L.ray_id = g - e.first;
   L.any = e.mode != 0;
-  return load_ray(e.rays, L.ray_id);
+  return load_ray_as<CS>(e.rays, L.ray_id);
 }
 RT_DEV void* out_of(const OneBatch& s, uint32_t) { return s.out; }
 RT_DEV void* out_of(const ManyBatches& s, uint32_t entry) { return s.table[entry].hits; }

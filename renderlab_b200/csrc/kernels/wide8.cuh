@@ -535,22 +535,23 @@ RT_DEV void w8_finish(const uint32_t* __restrict__ w, const W8View& V, W8Lane& L
   }
   void* __restrict__ out = out_of(src, L.entry);
   if (b.hit) w8_count<COUNT>(cnt, W8C_FINAL64);
+  // streaming stores (st.global.cs): the record is written once here and read once by the final pass
   if (LAYOUT == 1) {
     uint32_t* o = reinterpret_cast<uint32_t*>(out) + 5 * (size_t)id;
-    o[0] = __float_as_uint(b.t);
-    o[1] = b.hit ? ld(w, 8 + 24 * (size_t)b.inst + 21) + 1 : 0u;
-    o[2] = b.hit ? b.ident : 0u;
-    o[3] = b.hit ? b.inst : 0u;
-    o[4] = b.hit ? b.tri : 0u;
+    __stcs(o, __float_as_uint(b.t));
+    __stcs(o + 1, b.hit ? ld(w, 8 + 24 * (size_t)b.inst + 21) + 1 : 0u);
+    __stcs(o + 2, b.hit ? b.ident : 0u);
+    __stcs(o + 3, b.hit ? b.inst : 0u);
+    __stcs(o + 4, b.hit ? b.tri : 0u);
     return;
   }
   uint32_t* o = reinterpret_cast<uint32_t*>(out) + 10 * (size_t)id;
   if (!b.hit) {
-    o[0] = __float_as_uint(L.ray.tmax), o[1] = EMPTY, o[2] = o[3] = o[4] = 0;
-    o[5] = o[6] = 0, o[7] = o[8] = o[9] = 0;
+    __stcs(o, __float_as_uint(L.ray.tmax)), __stcs(o + 1, EMPTY);
+    for (int k = 2; k < 10; ++k) __stcs(o + k, 0u);
     return;
   }
-  o[0] = __float_as_uint(b.t), o[1] = b.inst, o[2] = b.tri;
+  __stcs(o, __float_as_uint(b.t)), __stcs(o + 1, b.inst), __stcs(o + 2, b.tri);
 }
 
 // t, u, v of the f64 reference's Möller-Trumbore (reference.rs:121-158) over the source triangle
@@ -590,8 +591,10 @@ __device__ __noinline__ bool mt64_values(const uint32_t* __restrict__ w, uint32_
 // primitive words and the world-space normal (unit_normal of the source winding, as gi_triangle's
 // caller forms it).
 template <uint32_t LAYOUT>
-RT_DEV void w8_final_hit(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t* __restrict__ o) {
-  if (LAYOUT == 1 ? o[1] == 0u : o[1] == EMPTY) return;  // a miss
+RT_DEV void w8_final_hit(const uint32_t* __restrict__ w, const W8View& V, const float4* __restrict__ rays, uint32_t i,
+                         uint32_t* __restrict__ o) {
+  if (LAYOUT == 1 ? o[1] == 0u : o[1] == EMPTY) return;  // a miss (its ray is not read)
+  const Ray ray = load_ray_cs(rays, i);
   const uint32_t inst = LAYOUT == 1 ? o[3] : o[1], tri = LAYOUT == 1 ? o[4] : o[2];
   const uint4 q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
   const uint32_t ident = q2.y, ref = q2.z;
@@ -627,7 +630,7 @@ __global__ void __launch_bounds__(256) k_wide8_final(const uint32_t* __restrict_
   const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   uint32_t* o = reinterpret_cast<uint32_t*>(src.out) + (LAYOUT == 1 ? 5 : 10) * (size_t)i;
-  w8_final_hit<LAYOUT>(w, V, load_ray(src.rays, i), o);
+  w8_final_hit<LAYOUT>(w, V, src.rays, i, o);
 }
 template <uint32_t LAYOUT>
 __global__ void __launch_bounds__(256) k_wide8_final(const uint32_t* __restrict__ w, W8View V, ManyBatches src, uint32_t n) {
@@ -643,7 +646,7 @@ __global__ void __launch_bounds__(256) k_wide8_final(const uint32_t* __restrict_
   if (e.mode != 0) return;
   const uint32_t i = g - e.first;
   uint32_t* o = reinterpret_cast<uint32_t*>(e.hits) + (LAYOUT == 1 ? 5 : 10) * (size_t)i;
-  w8_final_hit<LAYOUT>(w, V, load_ray(e.rays, i), o);
+  w8_final_hit<LAYOUT>(w, V, e.rays, i, o);
 }
 
 RT_DEV uint32_t octant_of(const F3& d) {
@@ -743,7 +746,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8_MIN_BLOCKS) k_wide8(const uint32_
       if ((want >> lane & 1u) && idx < n) id = idx;
     }
     if (id != EMPTY) {
-      L.ray = fetch(src, id, L);
+      L.ray = fetch<true>(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
       b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
@@ -924,7 +927,7 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
     L.phase = 0;
     bool live = id < n;  // the lane's ray still wants hits
     if (live) {
-      L.ray = fetch(src, id, L);
+      L.ray = fetch<true>(src, id, L);
       L.world_inv = safe_inverse(L.ray.d);
       W8Best& b = L.best;
       b.hit = false, b.has64 = false, b.t = L.ray.tmax, b.band = 0.0f, b.t64 = 0.0;
