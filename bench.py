@@ -288,12 +288,13 @@ def wide8_bytes(counters, layout, hit_bytes):
 # k_wide8 -- by (config, --small, kernel). Captured with
 #   ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum --clock-control none
 #       -k regex:^k_wide8$ -s 1 -c 1 python bench.py [--small] --steps 1 --warmup 3 --no-cpu --precision 0 --kernel wide8
-# (one pass; the launch is the first warm-up step's GI batch): precision-4M 1,061.5 MB read + 497.9 MB
-# written for 5,033,164 rays; the 1M-triangle reduced case 234.5 + 103.0 MB for 1,258,291 rays.
+# (one pass; the launch is the first warm-up step's GI batch): precision-4M 944.3 MB read + 451.2 MB
+# written for 5,033,164 rays; the 1M-triangle reduced case 234.5 + 103.0 MB for 1,258,291 rays (an
+# earlier build, before the walk's ray and hit streams took the evict-first form).
 # clusters-1M (--config 2 ... --kernel wide8p,wide8 --refill 8, -s 2: the first warm-up step's GI
-# batch): 580.6 MB read + 341.0 MB written for 4,194,304 rays.
-TRAFFIC = {(3, False, "k_wide8"): (1061.46e6 + 497.91e6) / 5_033_164, (3, True, "k_wide8"): (234.53e6 + 102.95e6) / 1_258_291,
-           (2, False, "k_wide8"): (580.62e6 + 341.04e6) / 4_194_304}
+# batch): 518.6 MB read + 319.8 MB written for 4,194,304 rays.
+TRAFFIC = {(3, False, "k_wide8"): (944.30e6 + 451.18e6) / 5_033_164, (3, True, "k_wide8"): (234.53e6 + 102.95e6) / 1_258_291,
+           (2, False, "k_wide8"): (518.57e6 + 319.81e6) / 4_194_304}
 
 
 def hit_bytes(layout, mode):
