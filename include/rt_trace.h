@@ -158,7 +158,8 @@ rt_status rt_scene_prepare(rt_ctx* ctx, rt_scene* scene, rt_kernel kernel);
  * box), then keeps the fastest, which the scene's later rt_scene_prepare calls also use, and
  * reports it in *chosen (0 for a scene without a top level, which is left as it is). Few large
  * instances favour 1 (each instance entered at its BLAS root); many small, deeply overlapping
- * ones favour more. Needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first; synchronous. No
+ * ones favour more. Needs rt_scene_prepare(scene, RT_KERNEL_WIDE8) first; synchronous; the
+ * scene's top level is rebuilt in place, so no other call may trace the scene meanwhile. No
  * counterpart in the reference, whose top level is the packed BVH4 over instance boxes
  * (src/instance_bvh.rs:162-460). */
 rt_status rt_scene_tune_top(rt_ctx* ctx, rt_scene* scene, const uint32_t* budgets, uint32_t n_budgets,
