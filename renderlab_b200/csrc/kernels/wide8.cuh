@@ -589,17 +589,15 @@ __device__ __noinline__ bool mt64_values(const uint32_t* __restrict__ w, uint32_
 
 // The final values of one closest hit (see the header): f64 t, u, v; for the GI layout also the
 // primitive words and the world-space normal (unit_normal of the source winding, as gi_triangle's
-// caller forms it).
+// caller forms it). The hit is on 8-wide triangle `tri` of instance `inst`; the walk has written
+// its record `o` (the identity words), and t_walk is the walk's t estimate.
 template <uint32_t LAYOUT>
-RT_DEV void w8_final_hit(const uint32_t* __restrict__ w, const W8View& V, const float4* __restrict__ rays, uint32_t i,
-                         uint32_t* __restrict__ o) {
-  if (LAYOUT == 1 ? o[1] == 0u : o[1] == EMPTY) return;  // a miss (its ray is not read)
-  const Ray ray = load_ray_cs(rays, i);
-  const uint32_t inst = LAYOUT == 1 ? o[3] : o[1], tri = LAYOUT == 1 ? o[4] : o[2];
+RT_DEV void w8_final_values(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray, uint32_t inst, uint32_t tri,
+                            float t_walk, uint32_t* __restrict__ o) {
   const uint4 q2 = __ldg(V.tris + 3 * (size_t)tri + 2);
   const uint32_t ident = q2.y, ref = q2.z;
   double t64, u64, v64;
-  float t = __uint_as_float(o[0]), u = 0.0f, v = 0.0f;
+  float t = t_walk, u = 0.0f, v = 0.0f;
   if (mt64_values<LAYOUT>(w, inst, ref, ray, t64, u64, v64)) t = (float)t64, u = (float)u64, v = (float)v64;
   if (LAYOUT == 1) {
     o[0] = __float_as_uint(t), o[3] = __float_as_uint(u), o[4] = __float_as_uint(v);
@@ -620,6 +618,23 @@ RT_DEV void w8_final_hit(const uint32_t* __restrict__ w, const W8View& V, const 
   else o[2] = ia, o[3] = ib, o[4] = ic;
   o[5] = __float_as_uint(u), o[6] = __float_as_uint(v);
   o[7] = __float_as_uint(nrm.x), o[8] = __float_as_uint(nrm.y), o[9] = __float_as_uint(nrm.z);
+}
+
+// The packet walk's form, out of line: called once a packet ends, it keeps the f64 work's
+// registers out of the walk's own allocation.
+template <uint32_t LAYOUT>
+__device__ __noinline__ void w8_final_values_call(const uint32_t* __restrict__ w, const W8View& V, const Ray& ray,
+                                                  uint32_t inst, uint32_t tri, float t_walk, uint32_t* __restrict__ o) {
+  w8_final_values<LAYOUT>(w, V, ray, inst, tri, t_walk, o);
+}
+
+// The final pass's form: the record at `o`, its ray read only for a hit.
+template <uint32_t LAYOUT>
+RT_DEV void w8_final_hit(const uint32_t* __restrict__ w, const W8View& V, const float4* __restrict__ rays, uint32_t i,
+                         uint32_t* __restrict__ o) {
+  if (LAYOUT == 1 ? o[1] == 0u : o[1] == EMPTY) return;  // a miss (its ray is not read)
+  const Ray ray = load_ray_cs(rays, i);
+  w8_final_values<LAYOUT>(w, V, ray, LAYOUT == 1 ? o[3] : o[1], LAYOUT == 1 ? o[4] : o[2], __uint_as_float(o[0]), o);
 }
 
 // The final pass after a closest-hit WIDE8 launch: one thread per ray of the launch's ray space
@@ -1007,7 +1022,15 @@ __global__ void __launch_bounds__(BLOCK, RT_W8P_MIN_BLOCKS) k_wide8_packet(const
         }
       }
     }
-    if (id < n) w8_finish<LAYOUT, AM, false>(w, V, L, src, nullptr);
+    if (id < n) {
+      w8_finish<LAYOUT, AM, false>(w, V, L, src, nullptr);
+      // The lanes of a warp end their packet together, so a closest hit's final values are made
+      // here, converged, rather than by a separate final pass (the same arithmetic on the same
+      // instance, triangle, ray and t estimate, hence the same words).
+      if (!any_of<AM>(L) && L.best.hit)
+        w8_final_values_call<LAYOUT>(w, V, L.ray, L.best.inst, L.best.tri, L.best.t,
+                                     reinterpret_cast<uint32_t*>(out_of(src, L.entry)) + (LAYOUT == 1 ? 5 : 10) * (size_t)L.ray_id);
+    }
   }
 }
 

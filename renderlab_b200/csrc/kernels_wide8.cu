@@ -207,7 +207,7 @@ cudaError_t launch_wide8_packet(const SceneView& s, uint32_t mode, const float4*
     e = mode == 0 ? run_packet(rtk::k_wide8_packet<1, 0, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream)
                   : run_packet(rtk::k_wide8_packet<1, 1, W8_BLOCK, OneBatch>, s.words, v, src, counter, n, st, stream);
   }
-  return then_final(e, mode == 0, s, v, src, n, stream);
+  return e;  // the packet walk makes its closest hits' final values itself
 }
 
 cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntry* table, uint32_t entries,
@@ -223,7 +223,7 @@ cudaError_t launch_wide8_packet_batches(const SceneView& s, const rtk::BatchEntr
   if (s.layout == 0) e = uniform_mode == 0 ? RT_W8P(0, 0) : (uniform_mode == 1 ? RT_W8P(0, 1) : RT_W8P(0, 2));
   else e = uniform_mode == 0 ? RT_W8P(1, 0) : (uniform_mode == 1 ? RT_W8P(1, 1) : RT_W8P(1, 2));
 #undef RT_W8P
-  return then_final(e, uniform_mode != 1, s, v, src, total, stream);
+  return e;  // the packet walk makes its closest hits' final values itself
 }
 
 }  // namespace rtl
